@@ -1,0 +1,45 @@
+"""Density-splat camera (src/core/camera.py of the reference), on libcnb.
+
+`Camera(n_steps, resolution, config)` and `capture(step, px_d, py_d, pz_d)`
+as in the reference (camera.py:10-48): clear the grid, build the orbiting
+MVP, splat, colourise.  The grid is [H, W] with W = config.RES_W or
+`resolution`, H = config.RES_H or `resolution`; the projection's aspect is
+W / H (the reference's square grid gives 1.0).  Frames stay on the device;
+the reference's host video buffer, PNG and ffmpeg output
+(camera.py:50-70) are not part of this package.
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _lib
+from ..utils.visualizer import colorize_frame, get_mvp_matrix
+
+
+class Camera:
+    def __init__(self, n_steps, resolution, config, device=None):
+        self.config = config
+        self.n = n_steps
+        self.width = int(getattr(config, "RES_W", None) or resolution)
+        self.height = int(getattr(config, "RES_H", None) or resolution)
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        self.grid_d = torch.zeros((self.height, self.width), dtype=torch.float32, device=dev)
+        self.box_center = (config.BOX_SIZE / 2, config.BOX_SIZE / 2, config.BOX_SIZE / 2)
+        self.mvp_d = torch.zeros((4, 4), dtype=torch.float32, device=dev)
+
+    def splat(self, step, px_d, py_d, pz_d):
+        """camera.py:40-44: clear, MVP, render_density.  Returns the grid."""
+        self.grid_d.zero_()
+        mvp = get_mvp_matrix(step, self.box_center, self.config.BOX_SIZE, self.config,
+                             aspect=self.width / self.height)
+        self.mvp_d.copy_(torch.from_numpy(mvp), non_blocking=False)
+        st = int(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.call("cnb_render_density", px_d.data_ptr(), py_d.data_ptr(), pz_d.data_ptr(),
+                  self.grid_d.data_ptr(), self.mvp_d.data_ptr(), px_d.shape[0], self.width,
+                  self.height, st)
+        return self.grid_d
+
+    def capture(self, step, px_d, py_d, pz_d):
+        """camera.py:29-48: splat and colourise; returns the [H, W, 3] frame."""
+        return colorize_frame(self.splat(step, px_d, py_d, pz_d))

@@ -1,0 +1,106 @@
+"""Simulation engine (src/core/engine.py of the reference), on libcnb.
+
+`SimulationEngine(config, state)` with `step()` and `run()` keeps the
+reference's sequence (engine.py:55-123): Hubble rate and time step on the
+host, Morton sort, tree build, forces, kick/drift, `a += da`.  Differences:
+the forces are one launch over all bodies (the reference launches 5 000
+bodies at a time), the step does not synchronise the device, and the force
+kernel is chosen by config.FORCE_MODE:
+
+  "reference"  per-particle stack traversal with the reference's opening
+               test (config.PRECISION "f64" = the reference's arithmetic,
+               "f32" = float32);
+  "grouped"    warp-per-bucket traversal (config.MAC "ref_x" or "periodic",
+               optional per-bucket theta from `theta_per_group`).
+
+Device error flags are read by `check()` (one synchronisation).
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _lib
+from .._arrays import check_status, status_buffer
+from ..utils.cosmology import get_hubble_param
+from .camera import Camera
+from .octree import OctreeManager
+
+MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC}
+
+
+class SimulationEngine:
+    def __init__(self, config, state, camera=True):
+        self.config = config
+        self.state = state
+        self.force_mode = getattr(config, "FORCE_MODE", "reference")
+        if self.force_mode not in ("reference", "grouped"):
+            raise ValueError("FORCE_MODE must be 'reference' or 'grouped'")
+        self.tree_manager = OctreeManager(state.n, config.TPB, device=state.device,
+                                          upward=getattr(config, "UPWARD", "plain"),
+                                          node_table=self.force_mode == "grouped")
+        res = getattr(config, "RES", 1024)
+        self.camera = Camera(config.N_STEPS, res, config, device=state.device) if camera else None
+        self.cache_size = getattr(config, "CACHE_SIZE", 256)
+        self.tpb = config.TPB
+        self.a = config.A_START
+        self.da = (config.A_END - config.A_START) / config.N_STEPS
+        self.top_nodes = torch.full((self.cache_size,), -1, dtype=torch.int32, device=state.device)
+        self.node_to_cache = torch.full((self.tree_manager.n_nodes,), -1, dtype=torch.int32,
+                                        device=state.device)
+        self.theta_per_group = None   # float32 [ceil(N/32)] device tensor, grouped mode only
+        self.stats = torch.zeros(2, dtype=torch.int64, device=state.device)
+        self.mac = MACS[getattr(config, "MAC", "ref_x")]
+        self.precision = _lib.PREC_F64 if getattr(config, "PRECISION", "f32") == "f64" else _lib.PREC_F32
+
+    def _stream(self):
+        return int(torch.cuda.current_stream(self.state.device).cuda_stream)
+
+    def compute_forces(self):
+        """The force stage of engine.py:91-111, one launch over all bodies."""
+        cfg, s, tm = self.config, self.state, self.tree_manager
+        st = self._stream()
+        status = status_buffer(s.device.index).data_ptr()
+        px, py, pz = s.pos
+        if self.force_mode == "grouped":
+            tpg = self.theta_per_group
+            _lib.call("cnb_forces_grouped", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                      tm.node_table.data_ptr(), s.force.data_ptr(), s.n, float(cfg.THETA),
+                      tpg.data_ptr() if tpg is not None else None, self.mac, float(cfg.G),
+                      float(cfg.SOFTENING), float(cfg.BOX_SIZE), self.stats.data_ptr(), status, st)
+        else:
+            _lib.call("cnb_compute_forces", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                      tm.child.data_ptr(), tm.mass.data_ptr(), tm.com.data_ptr(),
+                      tm.aabb_min.data_ptr(), tm.aabb_max.data_ptr(), s.force.data_ptr(),
+                      float(cfg.THETA), float(cfg.G), float(cfg.SOFTENING), float(cfg.BOX_SIZE),
+                      tm.root_idx.data_ptr(), 0, s.n, s.n, self.precision, status, st)
+
+    def step(self):
+        """engine.py:55-123."""
+        H = get_hubble_param(self.a, self.config)
+        dt_physics = self.da / (self.a * H) * 0.8
+        self.state.sort_buffer_by_morton(self.config)
+        self.tree_manager.build(self.state.pos, self.state.mass, self.state.codes)
+        self.compute_forces()
+        s = self.state
+        _lib.call("cnb_integrate", *(t.data_ptr() for t in s.pos + s.vel), s.force.data_ptr(), s.n,
+                  float(self.a), float(H), float(dt_physics), self._stream())
+        self.a += self.da
+
+    def run(self, n_steps=None, frames=False):
+        """engine.py:125-139 without the host video buffer: steps, captures a
+        frame per step, returns the last frame (or all frames if `frames`)."""
+        n_steps = self.config.N_STEPS if n_steps is None else n_steps
+        out = []
+        frame = None
+        for i in range(n_steps):
+            self.step()
+            if self.camera is not None:
+                frame = self.camera.capture(i, *self.state.pos)
+                if frames:
+                    out.append(frame.clone())
+        self.check()
+        return out if frames else frame
+
+    def check(self):
+        """Synchronise and raise CnbError if a kernel flagged an error."""
+        return check_status(self.state.device.index)

@@ -1,0 +1,81 @@
+"""Radix-tree manager (src/core/octree.py of the reference), on libcnb.
+
+`OctreeManager(n_bodies, tpb)` allocates the reference's buffers
+(octree.py:14-43); `build(pos_d, mass_d, codes_d)` runs reset, Karras build,
+upward pass, CoM normalisation and root search (octree.py:45-83) and returns
+`root_idx`; `get_buffers()` returns the reference's dict (octree.py:85-93).
+
+Options beyond the reference: `upward="compensated"` (two-sum float32 sums
+and a float64 root, `self.root_f64` = [mass, com x, y, z]), and
+`node_table=True`, which also builds the packed node table the grouped force
+traversal reads (`self.node_table`, [3, M, 4] float32).
+"""
+from __future__ import annotations
+
+import torch
+
+from .. import _lib
+from .._arrays import status_buffer
+
+
+class OctreeManager:
+    """octree.py:13-93."""
+
+    def __init__(self, n_bodies, tpb=256, device=None, upward="plain", node_table=False):
+        self.n = int(n_bodies)
+        self.n_nodes = max(2 * self.n - 1, 1)
+        self.tpb = tpb
+        self.bpg = (self.n + tpb - 1) // tpb
+        dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
+        m = self.n_nodes
+        self.child = torch.full((m, 2), -1, dtype=torch.int32, device=dev)
+        self.parent = torch.full((m,), -1, dtype=torch.int32, device=dev)
+        self.root_idx = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.mass = torch.zeros(m, dtype=torch.float32, device=dev)
+        self.com = torch.zeros((m, 3), dtype=torch.float32, device=dev)
+        self.aabb_min = torch.zeros((m, 3), dtype=torch.float32, device=dev)
+        self.aabb_max = torch.zeros((m, 3), dtype=torch.float32, device=dev)
+        self.counters = torch.zeros(m, dtype=torch.int32, device=dev)
+        if upward not in ("plain", "compensated"):
+            raise ValueError("upward must be 'plain' or 'compensated'")
+        self.upward = upward
+        self.err = torch.zeros((m, 4), dtype=torch.float32, device=dev) if upward == "compensated" else None
+        self.root_f64 = torch.zeros(4, dtype=torch.float64, device=dev)
+        self.node_table = torch.empty((3, m, 4), dtype=torch.float32, device=dev) if node_table else None
+
+    def _stream(self):
+        return int(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def build(self, pos_d, mass_d, codes_d):
+        """octree.py:45-83: reset, build_tree, compute_multipoles, normalize_com, find_root."""
+        st = self._stream()
+        n, m = self.n, self.n_nodes
+        status = status_buffer(self.device.index).data_ptr()
+        _lib.call("cnb_reset_tree_buffers", self.child.data_ptr(), self.parent.data_ptr(),
+                  self.counters.data_ptr(), self.root_idx.data_ptr(), m, st)
+        _lib.call("cnb_build_tree", codes_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(), n, st)
+        px, py, pz = pos_d
+        mode = _lib.UPWARD_COMPENSATED if self.upward == "compensated" else _lib.UPWARD_PLAIN
+        _lib.call("cnb_upward", px.data_ptr(), py.data_ptr(), pz.data_ptr(), mass_d.data_ptr(),
+                  self.child.data_ptr(), self.parent.data_ptr(), self.mass.data_ptr(),
+                  self.com.data_ptr(), self.aabb_min.data_ptr(), self.aabb_max.data_ptr(),
+                  self.err.data_ptr() if self.err is not None else None, self.counters.data_ptr(), n,
+                  mode, self.root_f64.data_ptr() if self.err is not None else None, status, st)
+        _lib.call("cnb_find_root", self.parent.data_ptr(), self.root_idx.data_ptr(), m, st)
+        if self.node_table is not None:
+            _lib.call("cnb_pack_nodes", self.mass.data_ptr(), self.com.data_ptr(),
+                      self.aabb_min.data_ptr(), self.aabb_max.data_ptr(), self.child.data_ptr(),
+                      self.node_table.data_ptr(), m, st)
+        return self.root_idx
+
+    def get_buffers(self):
+        """octree.py:85-93."""
+        return {
+            "child": self.child,
+            "mass": self.mass,
+            "com": self.com,
+            "min": self.aabb_min,
+            "max": self.aabb_max,
+            "root": self.root_idx,
+        }

@@ -1,0 +1,187 @@
+/*
+ * cnb.h -- C ABI of libcnb.so, the B200 (sm_100a) Barnes-Hut step.
+ *
+ * Each entry point replaces one Numba kernel (or CuPy call) of
+ * Cosmo-NBody; the comment above it cites the reference interface it
+ * stands in for.  Conventions:
+ *   - all array arguments are device pointers owned by the caller, in the
+ *     reference's layouts (SoA float32 positions/velocities, force [N,3]
+ *     row-major, children [M,2] int32, n_com/n_min/n_max [M,3] float32,
+ *     M = 2N-1 tree nodes: leaves 0..N-1, internal nodes N..2N-2);
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default);
+ *   - every call is asynchronous on `stream` and returns 0 or a negative
+ *     CNB_E_* code for argument or launch errors;
+ *   - kernels that can detect a bad state on the device OR CNB_FLAG_* bits
+ *     into `status` (one int32 in device memory, may be NULL); the caller
+ *     reads it after synchronising;
+ *   - no entry point allocates memory except cnb_ctx_create.
+ */
+#ifndef CNB_H
+#define CNB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes */
+#define CNB_OK 0
+#define CNB_E_INVALID_ARG (-1)
+#define CNB_E_CUDA (-2)
+#define CNB_E_NO_MEMORY (-3)
+#define CNB_E_TOO_LARGE (-4)
+#define CNB_E_DEVICE_FLAG (-5)
+
+/* device status bits */
+#define CNB_FLAG_STACK_OVERFLOW 1 /* traversal stack full: children dropped (reference: silent) */
+#define CNB_FLAG_BAD_TOPOLOGY 2   /* climb longer than the node count, or child index out of range */
+#define CNB_FLAG_NONFINITE 4      /* non-finite acceleration produced */
+#define CNB_FLAG_LIST_OVERFLOW 8  /* grouped traversal work queue exhausted */
+
+/* Morton key modes */
+#define CNB_KEY_COMPAT30 0 /* bit-exact with morton.py:13-63 (low 10 bits of each 21-bit coordinate) */
+#define CNB_KEY_MORTON63 1 /* full 21-bit interleave, coordinates clamped to [0, 2^21-1] */
+
+/* opening criteria */
+#define CNB_MAC_REF_X 0    /* physics_kernels.py:131-136: x-extent, clamped to box when > box/2 */
+#define CNB_MAC_PERIODIC 1 /* 3-D extent, and open any node whose image is ambiguous for a target */
+
+/* arithmetic of the per-particle traversal */
+#define CNB_PREC_F32 0
+#define CNB_PREC_F64 1 /* float64 like compiled Numba types physics_kernels.py:118-141 */
+
+/* upward pass modes */
+#define CNB_UPWARD_PLAIN 0       /* bit-exact with tree_kernels.py:131-214 */
+#define CNB_UPWARD_COMPENSATED 1 /* two-sum compensated float32 sums, float64 root */
+
+int cnb_version(void);
+const char *cnb_error_string(int code);
+/* Last CUDA error seen by the library on this host thread (cudaError_t value). */
+int cnb_last_cuda_error(void);
+/* Number of kernels this library has launched in this process. */
+int64_t cnb_launch_count(void);
+
+/* src/kernels/morton.py:65-90 compute_codes(pos_x, pos_y, pos_z, codes, indices, n_bodies).
+ * indices may be NULL. */
+int cnb_compute_codes(const float *x, const float *y, const float *z, uint64_t *codes,
+                      uint32_t *indices, int64_t n, int key_mode, void *stream);
+
+/* Scratch owner for the radix sort and the fused step. */
+typedef struct cnb_ctx cnb_ctx;
+int cnb_ctx_create(int64_t n_max, cnb_ctx **out);
+int cnb_ctx_destroy(cnb_ctx *ctx);
+
+/* src/core/state.py:35 `sort_idx = cp.argsort(codes)`: stable LSD radix
+ * sort of (key, index) pairs.  keys_out receives the sorted keys, perm_out
+ * the original index of each sorted key.  idx_in may be NULL (identity).
+ * key_bits = number of low key bits that may be non-zero (30 or 63). */
+int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
+                   const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
+                   void *stream);
+
+/* src/core/state.py:37-40 `a[sort_idx]` gathers: dst[k][i] = src[k][perm[i]]
+ * for k < n_arrays (at most 8 float32 arrays). */
+int cnb_gather_f32(const uint32_t *perm, int n_arrays, const float *const *src,
+                   float *const *dst, int64_t n, void *stream);
+
+/* src/kernels/tree_kernels.py:236-262 reset_tree_buffers(child, parent, counters, root_idx). */
+int cnb_reset_tree_buffers(int32_t *child, int32_t *parent, int32_t *counters,
+                           int32_t *root_idx, int64_t n_nodes, void *stream);
+
+/* src/kernels/tree_kernels.py:60-129 build_tree(codes, children, parents). */
+int cnb_build_tree(const uint64_t *codes, int32_t *children, int32_t *parents, int64_t n,
+                   void *stream);
+
+/* src/kernels/tree_kernels.py:131-191 compute_multipoles(pos_x, pos_y, pos_z, mass,
+ * children, parents, n_mass, n_com, n_min, n_max, counts).  n = bodies. */
+int cnb_compute_multipoles(const float *px, const float *py, const float *pz,
+                           const float *mass, const int32_t *children, const int32_t *parents,
+                           float *n_mass, float *n_com, float *n_min, float *n_max,
+                           int32_t *counts, int64_t n, int32_t *status, void *stream);
+
+/* Extended upward pass (no reference counterpart beyond tree_kernels.py:131-214):
+ * mode CNB_UPWARD_PLAIN reproduces compute_multipoles + normalize_com bit for
+ * bit; CNB_UPWARD_COMPENSATED carries a two-sum error term with every float32
+ * mass-weighted sum and sets the root's mass and CoM from a float64 reduction.
+ * Writes the normalised n_com.  n_err ([M,4] float32, 16-byte aligned) holds
+ * the compensation terms (compensated mode only, else may be NULL).
+ * root_f64 (device, 4 doubles: mass, CoM x, y, z; required in compensated
+ * mode, optional in plain mode, where the float32 tree is left untouched)
+ * receives the float64 root values.  counts must be zero on entry. */
+int cnb_upward(const float *px, const float *py, const float *pz, const float *mass,
+               const int32_t *children, const int32_t *parents, float *n_mass, float *n_com,
+               float *n_min, float *n_max, float *n_err, int32_t *counts, int64_t n, int mode,
+               double *root_f64, int32_t *status, void *stream);
+
+/* src/kernels/tree_kernels.py:193-214 normalize_com(n_mass, n_com, n_nodes). */
+int cnb_normalize_com(const float *n_mass, float *n_com, int64_t n_nodes, void *stream);
+
+/* src/kernels/tree_kernels.py:216-234 find_root(parents, root_idx). */
+int cnb_find_root(const int32_t *parents, int32_t *root_idx, int64_t n_nodes, void *stream);
+
+/* src/kernels/tree_kernels.py:264-313 build_top_tree_cache(child, root_idx, top_nodes,
+ * node_to_cache, cache_size).  node_to_cache must hold -1 for uncached nodes
+ * on entry (src/core/engine.py:81 fills it). */
+int cnb_build_top_tree_cache(const int32_t *child, const int32_t *root_idx,
+                             int32_t *top_nodes, int32_t *node_to_cache, int32_t cache_size,
+                             void *stream);
+
+/* src/kernels/physics_kernels.py:14-153 compute_forces(pos_x, pos_y, pos_z, children,
+ * n_mass, n_com, n_min, n_max, force, theta, G, soft, box, root, top_nodes,
+ * node_to_cache, off): per-particle stack traversal for targets
+ * off .. off+count-1 (n = bodies).  The top-tree cache only mirrors node data
+ * and is not needed.  precision: CNB_PREC_F64 follows the reference's
+ * float64 arithmetic, CNB_PREC_F32 computes in float32. */
+int cnb_compute_forces(const float *px, const float *py, const float *pz,
+                       const int32_t *children, const float *n_mass, const float *n_com,
+                       const float *n_min, const float *n_max, float *force, double theta,
+                       double G, double soft, double box, const int32_t *root_idx, int64_t off,
+                       int64_t count, int64_t n, int precision, int32_t *status, void *stream);
+
+/* src/kernels/physics_kernels.py:155-203 integrate(pos_x, pos_y, pos_z, vel_x, vel_y,
+ * vel_z, force, a, H, dt). */
+int cnb_integrate(float *px, float *py, float *pz, float *vx, float *vy, float *vz,
+                  const float *force, int64_t n, double a, double H, double dt, void *stream);
+
+/* src/kernels/render_kernels.py:12-47 render_density(pos_x, pos_y, pos_z, grid, mvp, res):
+ * grid is [height, width] float32 (width == height == res in the reference),
+ * mvp is a device float32[4,4]. */
+int cnb_render_density(const float *px, const float *py, const float *pz, float *grid,
+                       const float *mvp, int64_t n, int width, int height, void *stream);
+
+/* Node table for cnb_forces_grouped: three float4 arrays of n_nodes entries,
+ * back to back: (com, mass), (min, child0 bits), (max, child1 bits), built
+ * from the reference-layout tree (normalised n_com).  16-byte aligned. */
+int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
+                   const float *n_max, const int32_t *children, float *node_table,
+                   int64_t n_nodes, void *stream);
+
+/* The B200 form of src/kernels/physics_kernels.py:14-153: one warp per bucket
+ * of 32 Morton-consecutive bodies, shared-memory node stack and interaction
+ * list, float32 with rsqrt and per-pair minimum image.  theta_per_group
+ * (device, ceil(n/32) floats, may be NULL) overrides theta per bucket.  mac:
+ * CNB_MAC_REF_X or CNB_MAC_PERIODIC.  stats (device, 2 x uint64, may be
+ * NULL) accumulates [interactions, node tests]. */
+int cnb_forces_grouped(const float *px, const float *py, const float *pz,
+                       const float *node_table, float *force, int64_t n, double theta,
+                       const float *theta_per_group, int mac, double G, double soft, double box,
+                       unsigned long long *stats, int32_t *status, void *stream);
+
+/* Float64 minimum-image direct sum (the force law of
+ * src/kernels/physics_kernels.py:118-141 over every pair) for the bodies
+ * listed in targets (device int64[n_targets]); out is float64 [n_targets,3].
+ * Accuracy reference for the tree forces and labels for the learned
+ * opening-angle controller. */
+int cnb_direct_sum_f64(const float *px, const float *py, const float *pz, const float *mass,
+                       int64_t n, const int64_t *targets, int64_t n_targets, double G,
+                       double soft, double *out, void *stream);
+
+/* FP32 FMA throughput probe (no reference counterpart): `blocks` x 256
+ * threads, 16 * iters flops per thread; out holds blocks*256 floats. */
+int cnb_fma_probe(float *out, int64_t iters, int blocks, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CNB_H */

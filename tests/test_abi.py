@@ -1,0 +1,70 @@
+"""The C-ABI library loads and exports every symbol include/cnb.h declares
+(no compute calls: runs without a GPU)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "cnb.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(cnb_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "cnb_compute_codes" in names and "cnb_forces_grouped" in names
+    assert len(names) >= 20
+
+
+def test_library_exports_every_declared_symbol():
+    from cnb import _lib
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_binding_covers_header():
+    from cnb import _lib
+    assert set(declared_functions()) == set(_lib.SIGNATURES), \
+        set(declared_functions()) ^ set(_lib.SIGNATURES)
+
+
+def test_host_only_entry_points():
+    from cnb import _lib
+    lib = _lib.load()
+    assert lib.cnb_version() >= 1
+    assert lib.cnb_error_string(_lib.CNB_E_INVALID_ARG) == b"invalid argument"
+    # argument validation happens before any device work
+    assert lib.cnb_compute_codes(None, None, None, None, None, 10, 0, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_compute_codes(None, None, None, None, None, 0, 0, None) == _lib.CNB_OK
+    assert lib.cnb_compute_codes(None, None, None, None, None, -1, 0, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_build_tree(None, None, None, 5, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_forces_grouped(None, None, None, None, None, 5, 0.5, None, 7, 1.0, 0.01, 1.0,
+                                  None, None, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_sort_pairs(None, None, None, None, None, 5, 30, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_render_density(None, None, None, None, None, 4, 0, 4, None) == _lib.CNB_E_INVALID_ARG
+
+
+def test_launch_objects_validate_shape():
+    from cnb.kernels.morton import compute_codes
+    with pytest.raises(TypeError):
+        compute_codes(1, 2, 3)
+    with pytest.raises(TypeError):
+        compute_codes[1]
+    with pytest.raises(ValueError):
+        compute_codes[1, 2048]
+
+
+def test_launch_objects_reject_host_arrays():
+    import numpy as np
+    from cnb.kernels.morton import compute_codes
+    x = np.zeros(4, np.float32)
+    with pytest.raises(TypeError):
+        compute_codes[1, 256, 1](x, x, x, np.zeros(4, np.uint64), None, 4)
