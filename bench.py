@@ -1,0 +1,426 @@
+"""Barnes-Hut step benchmark: particle-steps/s at N = 128^3 on one B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the reference's full plain step at reference scale): 128^3 = 2,097,152
+float32 bodies from seeded Zel'dovich initial conditions (seed 1; P(k) ~ k^-2.5,
+sigma_disp = 0.3/128, a0 = 0.02, H0 = 67.8, Omega_m = 1, Omega_L = 0.692),
+theta = 0.5, softening 0.5/128, G = 1, kick-drift steps of da = 0.002, and the
+density splat to a 1920x1080 float32 grid with the orbiting 60-degree camera.
+One bench step = one simulation step (63-bit Morton keys, radix sort +
+permute, Karras build, upward pass, force traversal, kick/drift) plus the splat.
+
+`--impl ours` (default) runs libcnb on the GPU; `--impl reference` times the
+reference's algorithm (the CPU oracle restating src/kernels/*.py, all host
+threads) on the same workload, each step a bounded sample (all stages on all
+bodies except the force traversal, which runs on a fixed sample of targets
+and is scaled to N).  Under torchrun each rank runs an independent box
+(seed 1 + 1000 * rank: replicas, weak scaling); rank 0 prints the JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "cosmo-nbody_b200"))
+
+METRIC = "particle-steps/s at N=128^3 (full plain step + 1920x1080 splat)"
+N_GRID = 128
+FLOPS_PER_INTERACTION = 20   # 3 sub, 3 min-image, 5 d2, 1 +eps2, 1 rsqrt, 3 mul, 3 fma (+1)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n-grid", type=int, default=N_GRID)
+    ap.add_argument("--theta", type=float, default=0.5)
+    ap.add_argument("--force-mode", default="grouped", choices=["grouped", "reference"])
+    ap.add_argument("--mac", default="ref_x", choices=["ref_x", "periodic"])
+    ap.add_argument("--upward", default="plain", choices=["plain", "compensated"])
+    ap.add_argument("--width", type=int, default=1920)
+    ap.add_argument("--height", type=int, default=1080)
+    ap.add_argument("--accuracy-sample", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=8192)
+    ap.add_argument("--profile", action="store_true",
+                    help="timed loop only (no e2e, accuracy, CPU baseline or clock sampling)")
+    return ap.parse_args()
+
+
+def make_config(args, seed):
+    from cnb.utils import config as cfgmod
+    n = args.n_grid
+    return cfgmod.make(N_GRID=n, SOFTENING=0.5 / n, THETA=args.theta, N_STEPS=10,
+                       A_START=0.02, A_END=0.02 + 10 * 0.002, KEY_MODE="morton63",
+                       FORCE_MODE=args.force_mode, MAC=args.mac, PRECISION="f32",
+                       UPWARD=args.upward, RES=args.width, RES_W=args.width, RES_H=args.height,
+                       SEED=seed)
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return ws, rank, local
+
+
+def max_over_ranks(x, ws):
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    import torch
+    torch.cuda.synchronize()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or not self.path:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(s):
+            try:
+                return float(s)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def fma_peak_tflops():
+    """Measured FP32 FMA throughput (libcnb probe), TFLOP/s."""
+    import torch
+    from cnb import _lib
+    blocks = 148 * 16
+    out = torch.empty(blocks * 256, dtype=torch.float32, device="cuda")
+    iters = 20000
+    st = int(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        _lib.call("cnb_fma_probe", out.data_ptr(), iters, blocks, st)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib.call("cnb_fma_probe", out.data_ptr(), iters, blocks, st)
+        e1.record()
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        best = max(best, 16.0 * iters * blocks * 256 / (ms * 1e-3) / 1e12)
+    return best
+
+
+# ---------------------------------------------------------------- CPU (reference algorithm)
+
+def cpu_reference_step(pos, vel, mass, a, da, cfg, sample, threads):
+    """One step of the reference's algorithm on the host (oracle restating
+    src/core/engine.py:55-123 with the 63-bit key), forces on `sample`
+    evenly spaced targets scaled to N.  Returns (new pos, new vel, seconds)."""
+    from oracle import oracle as orc
+    n = pos[0].size
+    t0 = time.perf_counter()
+    H = orc.hubble(a)
+    dt = da / (a * H) * 0.8
+    spos, svel, smass, codes, _ = orc.sort_state(pos, vel, mass, orc.KEY_MORTON63)
+    ch, par = orc.build_tree(codes)
+    nm, nc, lo, hi = orc.compute_multipoles(*spos, smass, ch, par)
+    root = orc.find_root(par)
+    t1 = time.perf_counter()
+    targets = np.linspace(0, n - 1, min(sample, n)).astype(np.int64)
+    orc.forces_targets_f64(*spos, ch, nm, nc, lo, hi, cfg.THETA, cfg.G, cfg.SOFTENING,
+                           cfg.BOX_SIZE, root, targets, nthreads=threads)
+    t2 = time.perf_counter()
+    force = np.zeros((n, 3), np.float32)  # untimed stand-in for the unsampled targets
+    t3 = time.perf_counter()
+    new = orc.integrate(*spos, *svel, force, a, H, dt)
+    from cnb.utils.visualizer import get_mvp_matrix
+    mvp = get_mvp_matrix(0, (0.5, 0.5, 0.5), 1.0, cfg, aspect=cfg.RES_W / cfg.RES_H)
+    orc.render_density(*new[:3], mvp, cfg.RES_W, cfg.RES_H)
+    t4 = time.perf_counter()
+    seconds = (t1 - t0) + (t2 - t1) * n / targets.size + (t4 - t3)
+    return new[:3], new[3:], seconds
+
+
+def run_reference(args):
+    ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
+    if rank != 0:
+        return 0
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = make_config(args, 1)
+    n = cfg.N_BODIES
+    pos, vel = zeldovich_arrays(cfg.N_GRID, 1)
+    mass = np.full(n, 1.0 / n, np.float32)
+    threads = os.cpu_count() or 1
+    a = cfg.A_START
+    for _ in range(args.warmup):
+        cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads)
+    total = 0.0
+    for k in range(args.steps):
+        pos, vel, s = cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads)
+        a += 0.002
+        total += s
+    value = n * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Zel'dovich ICs)",
+        "config": config_dict(cfg, args),
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+                         "sample": f"all stages on all {n} bodies; force traversal on {args.cpu_sample} "
+                                   f"evenly spaced targets scaled to N"},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(cfg, args):
+    return {"workload": f"Zel'dovich {cfg.N_GRID}^3 plain Barnes-Hut step + {cfg.RES_W}x{cfg.RES_H} splat",
+            "n_bodies": cfg.N_BODIES, "theta": cfg.THETA, "softening": cfg.SOFTENING,
+            "da": 0.002, "a_start": cfg.A_START, "seed": 1, "keys": "morton63",
+            "force_mode": cfg.FORCE_MODE, "mac": cfg.MAC, "upward": cfg.UPWARD,
+            "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
+
+
+# ---------------------------------------------------------------- GPU
+
+def run_ours(args):
+    import torch
+    from cnb import _lib
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils.cosmology import zeldovich_arrays
+
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    seed = 1 + 1000 * rank
+    cfg = make_config(args, seed)
+    n = cfg.N_BODIES
+    pos_h, vel_h = zeldovich_arrays(cfg.N_GRID, seed)
+    state = SimulationState(n, pos_h, vel_h)
+    eng = SimulationEngine(cfg, state)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def one_step(i):
+        eng.step()
+        eng.camera.splat(i, *state.pos)
+
+    for i in range(args.warmup):
+        one_step(i)
+    eng.check()
+    barrier(ws)
+
+    eng.enable_stage_timing(True)
+    eng.stats.zero_()
+    launches0 = _lib.launch_count()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if not args.profile else None
+    if sampler:
+        sampler.__enter__()
+    barrier(ws)
+    for k in range(args.steps):
+        flush.zero_()
+        starts[k].record()
+        one_step(args.warmup + k)
+        ends[k].record()
+    barrier(ws)
+    if sampler:
+        sampler.__exit__()
+    launches = (_lib.launch_count() - launches0) // args.steps
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    stages = eng.stage_times()
+    eng.enable_stage_timing(False)
+    total_ms = max_over_ranks(sum(step_ms), ws)
+    stats = eng.stats.cpu().numpy()
+    eng.check()
+    value = ws * n * args.steps / (total_ms * 1e-3)
+    interactions_per_step = float(stats[0]) * 32 / args.steps   # list entries x 32 lanes
+    forces_ms = stages.get("forces", 0.0) / args.steps
+
+    line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Zel'dovich ICs)", "config": config_dict(cfg, args),
+            "gpu_launches": int(launches),
+            "stages_ms": {k: v / args.steps for k, v in stages.items()}}
+    if args.force_mode == "grouped":
+        line["interactions_per_body"] = interactions_per_step / n
+
+    if not args.profile:
+        peak = fma_peak_tflops()
+        achieved = interactions_per_step * FLOPS_PER_INTERACTION / (forces_ms * 1e-3) / 1e12
+        line["roofline"] = {"kernel": "k_forces_grouped", "bound": "fp32", "achieved": achieved,
+                            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                            "traffic": None,
+                            "note": "peak = measured FP32 FMA throughput (cnb_fma_probe); "
+                                    f"{FLOPS_PER_INTERACTION} flops per body-node interaction"}
+        line["clocks"] = sampler.summary()
+        line["accuracy"] = accuracy(eng, args)
+        line["e2e"] = e2e(eng, args, ws)
+        if rank == 0:
+            line["cpu_baseline"] = cpu_baseline(args)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def accuracy(eng, args):
+    """Median / p99 relative force error against the float64 minimum-image
+    direct sum on a seeded random sample of bodies, for the current state."""
+    import torch
+    from cnb import _lib
+    s = eng.state
+    eng.forces_only()
+    n = s.n
+    k = min(args.accuracy_sample, n)
+    targets = np.sort(np.random.default_rng(0).choice(n, k, replace=False)).astype(np.int64)
+    T = torch.from_numpy(targets).cuda()
+    out = torch.empty((k, 3), dtype=torch.float64, device="cuda")
+    st = int(torch.cuda.current_stream().cuda_stream)
+    _lib.call("cnb_direct_sum_f64", *(p.data_ptr() for p in s.pos), s.mass.data_ptr(), n, T.data_ptr(),
+              k, float(eng.config.G), float(eng.config.SOFTENING), out.data_ptr(), st)
+    ref = out.cpu().numpy()
+    got = s.force[T].double().cpu().numpy()
+    e = np.linalg.norm(got - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    rms = np.sqrt((np.linalg.norm(ref, axis=1) ** 2).mean())
+    en = np.linalg.norm(got - ref, axis=1) / rms
+    return {"vs": "float64 minimum-image direct sum", "sample": k, "median_rel": float(np.median(e)),
+            "p99_rel": float(np.percentile(e, 99)), "p99_rms_normalised": float(np.percentile(en, 99))}
+
+
+def e2e(eng, args, ws):
+    """The same step through the public API with host buffers: every step
+    copies positions and velocities in from pinned host memory and copies
+    positions, velocities and the density grid back."""
+    import torch
+    s = eng.state
+    n = s.n
+    host_in = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(6)]
+    for h, d in zip(host_in, s.pos + s.vel):
+        h.copy_(d)
+    host_out = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(6)]
+    grid_h = torch.empty(tuple(eng.camera.grid_d.shape), dtype=torch.float32, pin_memory=True)
+    steps = args.steps
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for k in range(steps):
+        for h, d in zip(host_in, s.pos + s.vel):
+            d.copy_(h, non_blocking=True)
+        eng.step()
+        eng.camera.splat(k, *s.pos)
+        for h, d in zip(host_out, s.pos + s.vel):
+            h.copy_(d, non_blocking=True)
+        grid_h.copy_(eng.camera.grid_d, non_blocking=True)
+    e1.record()
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    return {"value": ws * n * steps / (ms * 1e-3), "unit": "particle-steps/s",
+            "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 4 * grid_h.numel(),
+            "api": "cnb.core.engine.SimulationEngine.step + Camera.splat (libcnb C ABI)"}
+
+
+def cpu_baseline(args):
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = make_config(args, 1)
+    n = cfg.N_BODIES
+    pos, vel = zeldovich_arrays(cfg.N_GRID, 1)
+    mass = np.full(n, 1.0 / n, np.float32)
+    threads = os.cpu_count() or 1
+    _, _, s = cpu_reference_step(pos, vel, mass, cfg.A_START, 0.002, cfg, args.cpu_sample, threads)
+    return {"value": n / s, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"one step: all stages on all {n} bodies, force traversal (reference "
+                      f"per-body algorithm, float64) on {args.cpu_sample} evenly spaced targets "
+                      f"scaled to N"}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

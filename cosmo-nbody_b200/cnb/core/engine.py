@@ -51,6 +51,7 @@ class SimulationEngine:
         self.stats = torch.zeros(2, dtype=torch.int64, device=state.device)
         self.mac = MACS[getattr(config, "MAC", "ref_x")]
         self.precision = _lib.PREC_F64 if getattr(config, "PRECISION", "f32") == "f64" else _lib.PREC_F32
+        self.stage_events = None
 
     def _stream(self):
         return int(torch.cuda.current_stream(self.state.device).cuda_stream)
@@ -74,17 +75,49 @@ class SimulationEngine:
                       float(cfg.THETA), float(cfg.G), float(cfg.SOFTENING), float(cfg.BOX_SIZE),
                       tm.root_idx.data_ptr(), 0, s.n, s.n, self.precision, status, st)
 
+    def _mark(self, name):
+        if self.stage_events is not None:
+            ev = torch.cuda.Event(enable_timing=True)
+            ev.record()
+            self.stage_events.append((name, ev))
+
+    def forces_only(self):
+        """Sort, tree and forces for the current state (no integration)."""
+        self._mark("start")
+        self.state.sort_buffer_by_morton(self.config)
+        self._mark("sort")
+        self.tree_manager.build(self.state.pos, self.state.mass, self.state.codes)
+        self._mark("tree")
+        self.compute_forces()
+        self._mark("forces")
+
     def step(self):
         """engine.py:55-123."""
         H = get_hubble_param(self.a, self.config)
         dt_physics = self.da / (self.a * H) * 0.8
-        self.state.sort_buffer_by_morton(self.config)
-        self.tree_manager.build(self.state.pos, self.state.mass, self.state.codes)
-        self.compute_forces()
+        self.forces_only()
         s = self.state
         _lib.call("cnb_integrate", *(t.data_ptr() for t in s.pos + s.vel), s.force.data_ptr(), s.n,
                   float(self.a), float(H), float(dt_physics), self._stream())
+        self._mark("integrate")
         self.a += self.da
+
+    def enable_stage_timing(self, on=True):
+        """Record CUDA events between the stages of every step (stage_times() reads them)."""
+        self.stage_events = [] if on else None
+
+    def stage_times(self):
+        """Milliseconds per stage summed over the recorded steps; clears the record."""
+        out = {}
+        ev = self.stage_events or []
+        torch.cuda.synchronize()
+        for (a, ea), (b, eb) in zip(ev, ev[1:]):
+            if b == "start":
+                continue
+            out[b] = out.get(b, 0.0) + ea.elapsed_time(eb)
+        if self.stage_events is not None:
+            self.stage_events = []
+        return out
 
     def run(self, n_steps=None, frames=False):
         """engine.py:125-139 without the host video buffer: steps, captures a

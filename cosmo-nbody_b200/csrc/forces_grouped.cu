@@ -40,6 +40,7 @@ struct GroupedParams {
     float G, soft2, box;
     int mac;
     int64_t n;
+    int64_t m_nodes;
     int32_t root;
     int64_t n_groups;
     unsigned long long *stats;  // [0] interactions, [1] node tests (may be null)
@@ -81,6 +82,7 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
         const bool valid = i < P.n;
         const int64_t ii = valid ? i : g * 32;
         const float x = P.px[ii], y = P.py[ii], z = P.pz[ii];
+        if (valid && !(isfinite(x) && isfinite(y) && isfinite(z))) set_flag(P.status, CNB_FLAG_NONFINITE);
         // bucket bounding box (Morton buckets are compact; the wrap-around
         // of a bucket across the periodic boundary is handled by the
         // per-axis periodic distance below only when the box is < box/2)
@@ -105,7 +107,14 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
         if (lane == 0) stack[0] = P.root;
         top = 1;
         __syncwarp();
+        // a valid tree pushes every node at most once per bucket: more
+        // rounds than nodes means a cyclic topology
+        int64_t rounds = 0;
         while (top > 0) {
+            if (++rounds > P.m_nodes) {
+                if (lane == 0) set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
+                break;
+            }
             const int k = top < 32 ? top : 32;
             top -= k;
             int32_t node = -1;
@@ -114,6 +123,10 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
             bool accept = false, open = false;
             float4 A;
             int32_t c0 = -1, c1 = -1;
+            if (node >= P.m_nodes) {
+                set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
+                node = -1;
+            }
             if (node >= 0) {
                 A = __ldg(P.nA + node);
                 if (A.w > 0.f) {
@@ -261,6 +274,7 @@ extern "C" int cnb_forces_grouped(const float *px, const float *py, const float 
     P.box = (float)box;
     P.mac = mac;
     P.n = n;
+    P.m_nodes = m;
     P.root = n > 1 ? (int32_t)n : 0;
     P.n_groups = (n + 31) / 32;
     P.stats = stats;

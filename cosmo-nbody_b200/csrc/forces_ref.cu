@@ -53,13 +53,20 @@ __global__ void __launch_bounds__(128) k_forces_ref(
     if (i >= n) return;
     const int64_t m_nodes = 2 * n - 1;
     const float x = px[i], y = py[i], z = pz[i];
+    if (!(isfinite(x) && isfinite(y) && isfinite(z))) set_flag(status, CNB_FLAG_NONFINITE);
     T ax = 0, ay = 0, az = 0;
     int32_t stack[64];
     int top = 0;
     stack[top++] = __ldg(root_idx);
     bool overflow = false, bad = false;
     const T half_box = box * (T)0.5;
+    int64_t visits = 0;
     while (top > 0) {
+        // a valid tree visits every node at most once per target
+        if (++visits > m_nodes) {
+            bad = true;
+            break;
+        }
         const int32_t node = stack[--top];
         if (node < 0 || node >= m_nodes) {
             bad = true;
