@@ -50,6 +50,7 @@ SIGNATURES = {
     "cnb_ctx_create": (_int, [_i64, C.POINTER(_p)]),
     "cnb_ctx_destroy": (_int, [_p]),
     "cnb_sort_pairs": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
+    "cnb_sort_pairs_noalloc": (_int, [_p, _p, _p, _p, _i64, _int, _p]),
     "cnb_gather_f32": (_int, [_p, _int, _p, _p, _i64, _p]),
     "cnb_reset_tree_buffers": (_int, [_p, _p, _p, _p, _i64, _p]),
     "cnb_build_tree": (_int, [_p, _p, _p, _i64, _p]),

@@ -80,6 +80,21 @@ int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                    const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
                    void *stream);
 
+/* No counterpart in the reference.  The same stable (key, index) sort as
+ * cnb_sort_pairs for callers that cannot allocate device memory (a plugin
+ * whose host application owns all device memory through its own pool, or
+ * code running where a cudaMalloc and the synchronisation it may bring are
+ * not allowed).  It takes no context and allocates nothing: its scratch is a
+ * fixed device array inside libcnb.so, sized for at most
+ * CNB_NOALLOC_MAX_KEYS keys (about 24.3 MiB, held on every GPU that loads the
+ * library until the process exits).  Larger n returns CNB_E_TOO_LARGE.  The
+ * first call on a device looks up the array's device address (so make it
+ * before any stream capture).  All calls share the array: calls that overlap
+ * on the GPU race. */
+#define CNB_NOALLOC_MAX_KEYS (1 << 20)
+int cnb_sort_pairs_noalloc(const uint64_t *keys_in, uint64_t *keys_out, const uint32_t *idx_in,
+                           uint32_t *perm_out, int64_t n, int key_bits, void *stream);
+
 /* src/core/state.py:37-40 `a[sort_idx]` gathers: dst[k][i] = src[k][perm[i]]
  * for k < n_arrays (at most 8 float32 arrays). */
 int cnb_gather_f32(const uint32_t *perm, int n_arrays, const float *const *src,
