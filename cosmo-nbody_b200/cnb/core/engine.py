@@ -35,9 +35,11 @@ class SimulationEngine:
         self.force_mode = getattr(config, "FORCE_MODE", "reference")
         if self.force_mode not in ("reference", "grouped"):
             raise ValueError("FORCE_MODE must be 'reference' or 'grouped'")
+        self.bodies_per_lane = int(getattr(config, "BODIES_PER_LANE", 1))
         self.tree_manager = OctreeManager(state.n, config.TPB, device=state.device,
                                           upward=getattr(config, "UPWARD", "plain"),
-                                          node_table=self.force_mode == "grouped")
+                                          node_table=self.force_mode == "grouped",
+                                          bucket=32 * self.bodies_per_lane)
         res = getattr(config, "RES", 1024)
         self.camera = Camera(config.N_STEPS, res, config, device=state.device) if camera else None
         self.cache_size = getattr(config, "CACHE_SIZE", 256)
@@ -47,9 +49,12 @@ class SimulationEngine:
         self.top_nodes = torch.full((self.cache_size,), -1, dtype=torch.int32, device=state.device)
         self.node_to_cache = torch.full((self.tree_manager.n_nodes,), -1, dtype=torch.int32,
                                         device=state.device)
-        self.theta_per_group = None   # float32 [ceil(N/32)] device tensor, grouped mode only
+        self.theta_per_group = None   # float32 per bucket slot (device), grouped mode only
         self.stats = torch.zeros(2, dtype=torch.int64, device=state.device)
         self.mac = MACS[getattr(config, "MAC", "ref_x")]
+        # periodic test: image-ambiguous nodes of at most SLAB_BODIES bodies' mass are applied
+        # with the per-pair minimum image (0 = exact)
+        self.slab_mass = float(getattr(config, "SLAB_BODIES", 0)) / max(state.n, 1)
         self.precision = _lib.PREC_F64 if getattr(config, "PRECISION", "f32") == "f64" else _lib.PREC_F32
         self.stage_events = None
 
@@ -65,9 +70,10 @@ class SimulationEngine:
         if self.force_mode == "grouped":
             tpg = self.theta_per_group
             _lib.call("cnb_forces_grouped", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
-                      tm.node_table.data_ptr(), s.force.data_ptr(), s.n, float(cfg.THETA),
-                      tpg.data_ptr() if tpg is not None else None, self.mac, float(cfg.G),
-                      float(cfg.SOFTENING), float(cfg.BOX_SIZE), self.stats.data_ptr(), status, st)
+                      tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,
+                      float(cfg.THETA), tpg.data_ptr() if tpg is not None else None, self.mac,
+                      self.bodies_per_lane, float(cfg.G), float(cfg.SOFTENING),
+                      float(cfg.BOX_SIZE), self.slab_mass, self.stats.data_ptr(), status, st)
         else:
             _lib.call("cnb_compute_forces", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                       tm.child.data_ptr(), tm.mass.data_ptr(), tm.com.data_ptr(),

@@ -7,8 +7,9 @@ upward pass, CoM normalisation and root search (octree.py:45-83) and returns
 
 Options beyond the reference: `upward="compensated"` (two-sum float32 sums
 and a float64 root, `self.root_f64` = [mass, com x, y, z]), and
-`node_table=True`, which also builds the packed node table the grouped force
-traversal reads (`self.node_table`, [3, M, 4] float32).
+`node_table=True`, which also builds what the grouped force traversal reads:
+the node table (`self.node_table`, [4, M, 4] float32), the node ranges and
+the bucket table (`self.workspace`, buckets of at most `bucket` bodies).
 """
 from __future__ import annotations
 
@@ -21,7 +22,8 @@ from .._arrays import status_buffer
 class OctreeManager:
     """octree.py:13-93."""
 
-    def __init__(self, n_bodies, tpb=256, device=None, upward="plain", node_table=False):
+    def __init__(self, n_bodies, tpb=256, device=None, upward="plain", node_table=False,
+                 bucket=32):
         self.n = int(n_bodies)
         self.n_nodes = max(2 * self.n - 1, 1)
         self.tpb = tpb
@@ -42,7 +44,13 @@ class OctreeManager:
         self.upward = upward
         self.err = torch.zeros((m, 4), dtype=torch.float32, device=dev) if upward == "compensated" else None
         self.root_f64 = torch.zeros(4, dtype=torch.float64, device=dev)
-        self.node_table = torch.empty((3, m, 4), dtype=torch.float32, device=dev) if node_table else None
+        self.node_table = None
+        if node_table:
+            # traversal records and boxes, node ranges and the bucket table
+            self.node_table = torch.empty((4, m, 4), dtype=torch.float32, device=dev)
+            self.ranges = torch.zeros((max(self.n - 1, 1), 2), dtype=torch.int32, device=dev)
+            self.workspace = torch.zeros(4 + 2 * max(self.n, 1), dtype=torch.int32, device=dev)
+            self.bucket = int(bucket)
 
     def _stream(self):
         return int(torch.cuda.current_stream(self.device).cuda_stream)
@@ -54,7 +62,11 @@ class OctreeManager:
         status = status_buffer(self.device.index).data_ptr()
         _lib.call("cnb_reset_tree_buffers", self.child.data_ptr(), self.parent.data_ptr(),
                   self.counters.data_ptr(), self.root_idx.data_ptr(), m, st)
-        _lib.call("cnb_build_tree", codes_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(), n, st)
+        if self.node_table is not None:
+            _lib.call("cnb_build_tree_ranges", codes_d.data_ptr(), self.child.data_ptr(),
+                      self.parent.data_ptr(), self.ranges.data_ptr(), n, st)
+        else:
+            _lib.call("cnb_build_tree", codes_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(), n, st)
         px, py, pz = pos_d
         mode = _lib.UPWARD_COMPENSATED if self.upward == "compensated" else _lib.UPWARD_PLAIN
         _lib.call("cnb_upward", px.data_ptr(), py.data_ptr(), pz.data_ptr(), mass_d.data_ptr(),
@@ -67,6 +79,8 @@ class OctreeManager:
             _lib.call("cnb_pack_nodes", self.mass.data_ptr(), self.com.data_ptr(),
                       self.aabb_min.data_ptr(), self.aabb_max.data_ptr(), self.child.data_ptr(),
                       self.node_table.data_ptr(), m, st)
+            _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), n,
+                      self.bucket, self.workspace.data_ptr(), st)
         return self.root_idx
 
     def get_buffers(self):

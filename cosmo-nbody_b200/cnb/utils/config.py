@@ -41,7 +41,9 @@ FORCE_MODE = "reference"   # "reference": per-particle stack traversal; "grouped
 MAC = "ref_x"              # "ref_x": reference opening test; "periodic": 3-D extent + image-safe opening
 PRECISION = "f32"          # per-particle traversal arithmetic: "f32" or "f64" (the reference's)
 UPWARD = "plain"           # "plain": bit-exact upward pass; "compensated": two-sum + float64 root
-BUCKET = 32                # bodies per leaf group in the grouped traversal
+BODIES_PER_LANE = 1        # grouped traversal: bodies per lane (buckets of 32 x this)
+SLAB_BODIES = 0            # periodic test: image-ambiguous nodes up to this many bodies' mass are
+                           # applied with the per-pair minimum image (0 = exact)
 SEED = 0                   # initial-condition seed
 RES_W = None               # render width (None: RES)
 RES_H = None               # render height (None: RES)

@@ -9,7 +9,7 @@ struct cnb_ctx {
     int64_t tiles_max = 0;
     uint64_t *keys_tmp[2] = {nullptr, nullptr};
     uint32_t *vals_tmp[2] = {nullptr, nullptr};
-    uint32_t *tile_hist = nullptr;  // [256 * tiles_max] digit-major
+    uint32_t *tile_hist = nullptr;  // [256 * (tiles_max + 1)]: digit-major counts, digit totals
     // grouped traversal scratch (grown on demand by cnb_forces_grouped)
     void *group_scratch = nullptr;
     size_t group_scratch_bytes = 0;

@@ -1,71 +1,95 @@
 // forces_grouped.cu -- warp-cooperative Barnes-Hut traversal over
-// Morton-contiguous leaf buckets (the B200 form of
+// Morton-contiguous buckets (the B200 form of
 // src/kernels/physics_kernels.py:14-153).
 //
-// One warp per bucket of 32 consecutive (Morton-sorted) bodies.  The warp
-// walks the tree 32 nodes at a time from a per-warp node stack in shared
-// memory: each lane tests one node against the bucket's bounding box, the
-// accepted nodes (and reached leaves) are appended to a per-warp interaction
-// list in shared memory with one ballot, and the opened nodes push their two
-// children.  Whenever the list holds 32 entries every lane applies all of
-// them to its own body (float32, rsqrt, per-pair minimum image), so the
-// force loop reads shared memory only and runs without divergence.
+// A bucket is a maximal radix-tree subtree with at most 32*BPL bodies
+// (cnb_make_buckets), so it is contiguous in the sorted order and spatially
+// compact.  One warp takes a bucket (dynamic scheduling: an atomic work
+// counter), each lane holds BPL bodies.  The warp walks the tree 32 nodes at
+// a time from a per-warp node stack in shared memory: each lane tests one
+// node against the bucket's bounding box, accepted nodes (and reached
+// leaves) are appended to a per-warp interaction list in shared memory with
+// one ballot, opened nodes push their two children.  Whenever the list holds
+// 32 entries, every lane applies them to its bodies: float32, rsqrt, and the
+// per-pair minimum image only for entries whose image can differ between the
+// bucket's bodies (flagged by a negative mass), so the force loop reads
+// shared memory only and never diverges.
 //
-// Opening tests (bucket box B, node CoM image c nearest the bucket centre,
-// dmin = periodic distance from c to B, per axis):
+// Opening tests (bucket box B with centre g and half-size h, node CoM image c
+// nearest g, dmin = periodic distance from c to B, per axis):
 //   CNB_MAC_REF_X:    open unless leaf or sx^2 < theta^2 dmin^2, sx the node's
 //                     x-extent set to `box` above box/2 (physics_kernels.py:131-136).
-//                     Every node the bucket accepts, each of its bodies would
-//                     accept in the reference traversal (dmin <= |d|).
-//   CNB_MAC_PERIODIC: 3-D extent l; also open any node whose image is not the
-//                     same for every (body, node member) pair, so the monopole
-//                     of an accepted node is applied at one consistent image.
-// theta can be one value or one per bucket (learned controller).
+//                     Each node the bucket accepts, every one of its bodies
+//                     would accept in the reference traversal (dmin <= |d|).
+//   CNB_MAC_PERIODIC: 3-D extent l; also open any node whose members' image is
+//                     not the same for every body of the bucket, so an accepted
+//                     monopole is applied at one consistent image -- unless the
+//                     node's mass is at most slab_mass, when it is applied with
+//                     the per-pair minimum image of its CoM.  slab_mass = 0 is
+//                     exact; a small positive value bounds the cost of the
+//                     sources near the plane antipodal to the bucket.
+// theta is one value or one per bucket (learned controller).
 #include "common.cuh"
 
 namespace cnb {
 
-constexpr int kGWarps = 4;           // warps per block
-constexpr int kGStack = 2048;        // node stack entries per warp
-constexpr int kGList = 64;           // interaction list entries per warp
+constexpr int kGWarps = 4;     // warps per block
+constexpr int kGStack = 2048;  // node stack entries per warp
+constexpr int kGList = 64;     // interaction list entries per warp
 
 struct GroupedParams {
     const float *px, *py, *pz;
-    const float4 *nA;  // (com x, y, z, mass)
-    const float4 *nB;  // (min x, y, z, child0 bits)
-    const float4 *nC;  // (max x, y, z, child1 bits)
-    float *force;      // [N,3]
-    const float *theta_per_group;  // may be null
+    const float4 *rec;   // [2*M]: (com, mass), (x-extent, 3-D extent, child0 bits, child1 bits)
+    const float4 *aabb;  // [2*M]: (min, 0), (max, 0)
+    float *force;        // [N,3]
+    int32_t *ws;         // [0] bucket count, [1] work counter, [2] max stack depth
+    const int2 *buckets; // (first body, count)
+    const float *theta_per_bucket;  // may be null
     float theta;
     float G, soft2, box;
+    float slab_mass;  // CNB_MAC_PERIODIC: image-ambiguous nodes up to this mass are accepted
     int mac;
     int64_t n;
     int64_t m_nodes;
     int32_t root;
-    int64_t n_groups;
-    unsigned long long *stats;  // [0] interactions, [1] node tests (may be null)
+    // many boxes in one tree (boxes.cu): box = codes[first body] >> box_shift
+    const uint64_t *codes;      // null: one box
+    int box_shift;
+    const int32_t *box_roots;   // subtree root per box
+    const float4 *box_params;   // (theta, softening, slab mass, 0) per box
+    unsigned long long *stats;  // [0] body-entry interactions, [1] node tests (may be null)
     int32_t *status;
 };
 
-__device__ __forceinline__ void apply_list(const float4 *list, int cnt, float x, float y,
-                                           float z, float soft2, float &ax, float &ay,
-                                           float &az) {
-#pragma unroll 8
+template <int BPL>
+__device__ __forceinline__ void apply_list(const float4 *list, int cnt, const float (&x)[BPL],
+                                           const float (&y)[BPL], const float (&z)[BPL],
+                                           float soft2, float (&ax)[BPL], float (&ay)[BPL],
+                                           float (&az)[BPL]) {
+#pragma unroll 4
     for (int j = 0; j < cnt; ++j) {
         const float4 e = list[j];
-        float dx = e.x - x, dy = e.y - y, dz = e.z - z;
-        dx -= rintf(dx);
-        dy -= rintf(dy);
-        dz -= rintf(dz);
-        const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-        const float r = rsqrtf(d2 + soft2);
-        const float f = (d2 > 1e-7f) ? e.w * r * r * r : 0.f;
-        ax = fmaf(f, dx, ax);
-        ay = fmaf(f, dy, ay);
-        az = fmaf(f, dz, az);
+        const bool wrap = e.w < 0.f;  // same entry in every lane: uniform branch
+        const float m = fabsf(e.w);
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) {
+            float dx = e.x - x[b], dy = e.y - y[b], dz = e.z - z[b];
+            if (wrap) {
+                dx -= rintf(dx);
+                dy -= rintf(dy);
+                dz -= rintf(dz);
+            }
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const float r = rsqrtf(d2 + soft2);
+            const float f = (d2 > 1e-7f) ? m * r * r * r : 0.f;
+            ax[b] = fmaf(f, dx, ax[b]);
+            ay[b] = fmaf(f, dy, ay[b]);
+            az[b] = fmaf(f, dz, az[b]);
+        }
     }
 }
 
+template <int BPL>
 __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P) {
     __shared__ int32_t s_stack[kGWarps][kGStack];
     __shared__ float4 s_list[kGWarps][kGList];
@@ -73,20 +97,38 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
     const uint32_t lt = (1u << lane) - 1u;
     int32_t *stack = s_stack[wib];
     float4 *list = s_list[wib];
-    unsigned long long n_inter = 0, n_tests = 0;
+    unsigned long long n_tests = 0;
+    int max_top = 0;
     bool overflow = false;
+    const int n_buckets = P.ws[0];
+    const float half_box = 0.5f * P.box;
 
-    for (int64_t g = (int64_t)blockIdx.x * kGWarps + wib; g < P.n_groups;
-         g += (int64_t)gridDim.x * kGWarps) {
-        const int64_t i = g * 32 + lane;
-        const bool valid = i < P.n;
-        const int64_t ii = valid ? i : g * 32;
-        const float x = P.px[ii], y = P.py[ii], z = P.pz[ii];
-        if (valid && !(isfinite(x) && isfinite(y) && isfinite(z))) set_flag(P.status, CNB_FLAG_NONFINITE);
-        // bucket bounding box (Morton buckets are compact; the wrap-around
-        // of a bucket across the periodic boundary is handled by the
-        // per-axis periodic distance below only when the box is < box/2)
-        float lx = x, ly = y, lz = z, hx = x, hy = y, hz = z;
+    for (;;) {
+        int g = 0;
+        if (lane == 0) g = atomicAdd(P.ws + 1, 1);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= n_buckets) break;
+        const int2 bk = P.buckets[g];
+        const int count = bk.y;
+        float x[BPL], y[BPL], z[BPL];
+        bool valid[BPL];
+        float lx = INFINITY, ly = INFINITY, lz = INFINITY;
+        float hx = -INFINITY, hy = -INFINITY, hz = -INFINITY;
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) {
+            const int k = lane + 32 * b;
+            valid[b] = k < count;
+            const int64_t i = (int64_t)bk.x + (valid[b] ? k : 0);
+            x[b] = P.px[i];
+            y[b] = P.py[i];
+            z[b] = P.pz[i];
+            if (valid[b]) {
+                if (!(isfinite(x[b]) && isfinite(y[b]) && isfinite(z[b])))
+                    set_flag(P.status, CNB_FLAG_NONFINITE);
+                lx = fminf(lx, x[b]); ly = fminf(ly, y[b]); lz = fminf(lz, z[b]);
+                hx = fmaxf(hx, x[b]); hy = fmaxf(hy, y[b]); hz = fmaxf(hz, z[b]);
+            }
+        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             lx = fminf(lx, __shfl_xor_sync(0xffffffffu, lx, o));
@@ -98,17 +140,30 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
         }
         const float gcx = 0.5f * (lx + hx), gcy = 0.5f * (ly + hy), gcz = 0.5f * (lz + hz);
         const float ghx = 0.5f * (hx - lx), ghy = 0.5f * (hy - ly), ghz = 0.5f * (hz - lz);
-        const float th = P.theta_per_group ? P.theta_per_group[g] : P.theta;
+        // an entry whose image offset from the centre stays below this needs no per-pair wrap
+        const float wlx = 0.5f - ghx - 1e-6f, wly = 0.5f - ghy - 1e-6f, wlz = 0.5f - ghz - 1e-6f;
+        float th = P.theta, soft2 = P.soft2, slab_mass = P.slab_mass;
+        int32_t root = P.root;
+        if (P.box_roots) {
+            const uint64_t b = P.codes[bk.x] >> P.box_shift;
+            const float4 bp = P.box_params[b];
+            root = P.box_roots[b];
+            th = bp.x;
+            soft2 = bp.y * bp.y;
+            slab_mass = bp.z;
+        }
+        if (P.theta_per_bucket) th = P.theta_per_bucket[g];
         const float th2 = th * th;
-        const float half_box = 0.5f * P.box;
 
-        float ax = 0.f, ay = 0.f, az = 0.f;
-        int top = 0, cnt = 0;
-        if (lane == 0) stack[0] = P.root;
-        top = 1;
+        float ax[BPL], ay[BPL], az[BPL];
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) ax[b] = ay[b] = az[b] = 0.f;
+        int top = 1, cnt = 0;
+        unsigned long long n_entries = 0;
+        if (lane == 0) stack[0] = root;
         __syncwarp();
-        // a valid tree pushes every node at most once per bucket: more
-        // rounds than nodes means a cyclic topology
+        // a valid tree pushes every node at most once per bucket: more rounds
+        // than nodes means a cyclic topology
         int64_t rounds = 0;
         while (top > 0) {
             if (++rounds > P.m_nodes) {
@@ -120,57 +175,63 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
             int32_t node = -1;
             if (lane < k) node = stack[top + lane];
             __syncwarp();
-            bool accept = false, open = false;
-            float4 A;
-            int32_t c0 = -1, c1 = -1;
             if (node >= P.m_nodes) {
                 set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
                 node = -1;
             }
+            bool accept = false, open = false, consistent = true;
+            float4 E = make_float4(0.f, 0.f, 0.f, 0.f);
+            int32_t c0 = -1, c1 = -1;
             if (node >= 0) {
-                A = __ldg(P.nA + node);
+                const float4 A = __ldg(P.rec + 2 * node);
                 if (A.w > 0.f) {
-                    const float4 B = __ldg(P.nB + node);
-                    const float4 C = __ldg(P.nC + node);
-                    c0 = __float_as_int(B.w);
-                    c1 = __float_as_int(C.w);
+                    const float4 S = __ldg(P.rec + 2 * node + 1);
+                    c0 = __float_as_int(S.z);
+                    c1 = __float_as_int(S.w);
+                    float dx = A.x - gcx, dy = A.y - gcy, dz = A.z - gcz;
+                    const float sx_ = rintf(dx), sy_ = rintf(dy), sz_ = rintf(dz);
+                    dx -= sx_;
+                    dy -= sy_;
+                    dz -= sz_;
                     if (c0 == -1) {
                         accept = true;
                     } else {
-                        float dx = A.x - gcx, dy = A.y - gcy, dz = A.z - gcz;
-                        const float sx_ = rintf(dx), sy_ = rintf(dy), sz_ = rintf(dz);
-                        dx -= sx_;
-                        dy -= sy_;
-                        dz -= sz_;
                         const float tx = fmaxf(fabsf(dx) - ghx, 0.f);
                         const float ty = fmaxf(fabsf(dy) - ghy, 0.f);
                         const float tz = fmaxf(fabsf(dz) - ghz, 0.f);
                         const float d2min = tx * tx + ty * ty + tz * tz;
                         if (P.mac == CNB_MAC_REF_X) {
-                            float s = C.x - B.x;
-                            s = s > half_box ? P.box : s;
+                            const float s = S.x > half_box ? P.box : S.x;
                             accept = s * s < th2 * d2min;
-                        } else {
+                        } else if (S.y * S.y < th2 * d2min) {
                             // node box at the image chosen for its CoM
-                            const float ex = fmaxf(C.x - sx_, hx) - fminf(B.x - sx_, lx);
-                            const float ey = fmaxf(C.y - sy_, hy) - fminf(B.y - sy_, ly);
-                            const float ez = fmaxf(C.z - sz_, hz) - fminf(B.z - sz_, lz);
-                            const bool consistent = ex < half_box && ey < half_box && ez < half_box;
-                            const float l = fmaxf(C.x - B.x, fmaxf(C.y - B.y, C.z - B.z));
-                            accept = consistent && (l * l < th2 * d2min);
+                            const float4 lo = __ldg(P.aabb + 2 * node);
+                            const float4 hi = __ldg(P.aabb + 2 * node + 1);
+                            const float ex = fmaxf(hi.x - sx_, hx) - fminf(lo.x - sx_, lx);
+                            const float ey = fmaxf(hi.y - sy_, hy) - fminf(lo.y - sy_, ly);
+                            const float ez = fmaxf(hi.z - sz_, hz) - fminf(lo.z - sz_, lz);
+                            consistent = ex < half_box && ey < half_box && ez < half_box;
+                            // a light image-ambiguous node is applied with the
+                            // per-pair minimum image of its CoM (bounded error)
+                            accept = consistent || A.w <= slab_mass;
                         }
                         open = !accept;
+                    }
+                    if (accept) {
+                        const bool same_image = consistent &&
+                            fabsf(dx) < wlx && fabsf(dy) < wly && fabsf(dz) < wlz;
+                        E = make_float4(A.x - sx_, A.y - sy_, A.z - sz_, same_image ? A.w : -A.w);
                     }
                 }
             }
             n_tests += (node >= 0);
             const uint32_t am = __ballot_sync(0xffffffffu, accept);
             const uint32_t om = __ballot_sync(0xffffffffu, open);
-            if (accept) list[cnt + __popc(am & lt)] = A;
+            if (accept) list[cnt + __popc(am & lt)] = E;
             cnt += __popc(am);
             const int nopen = __popc(om);
             if (top + 2 * nopen > kGStack) {
-                overflow = true;  // drop the children (flagged)
+                overflow = true;  // children dropped (flagged)
             } else {
                 if (open) {
                     const int pos = top + 2 * __popc(om & lt);
@@ -178,53 +239,63 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
                     stack[pos + 1] = c0;
                 }
                 top += 2 * nopen;
+                max_top = max(max_top, top);
             }
             __syncwarp();
             if (cnt >= 32) {
-                apply_list(list, 32, x, y, z, P.soft2, ax, ay, az);
-                n_inter += 32;
+                apply_list<BPL>(list, 32, x, y, z, soft2, ax, ay, az);
+                n_entries += 32;
                 __syncwarp();
                 if (lane < cnt - 32) list[lane] = list[32 + lane];
                 cnt -= 32;
                 __syncwarp();
             }
         }
-        apply_list(list, cnt, x, y, z, P.soft2, ax, ay, az);
-        n_inter += cnt;
+        apply_list<BPL>(list, cnt, x, y, z, soft2, ax, ay, az);
+        n_entries += cnt;
         __syncwarp();
-        if (valid) {
-            const float fx = P.G * ax, fy = P.G * ay, fz = P.G * az;
-            P.force[3 * i] = fx;
-            P.force[3 * i + 1] = fy;
-            P.force[3 * i + 2] = fz;
-            if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz)) set_flag(P.status, CNB_FLAG_NONFINITE);
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) {
+            if (valid[b]) {
+                const int64_t i = (int64_t)bk.x + lane + 32 * b;
+                const float fx = P.G * ax[b], fy = P.G * ay[b], fz = P.G * az[b];
+                P.force[3 * i] = fx;
+                P.force[3 * i + 1] = fy;
+                P.force[3 * i + 2] = fz;
+                if (!isfinite(fx) || !isfinite(fy) || !isfinite(fz))
+                    set_flag(P.status, CNB_FLAG_NONFINITE);
+            }
         }
+        if (P.stats && lane == 0) atomicAdd(P.stats, n_entries * (unsigned long long)count);
     }
     if (overflow && lane == 0) set_flag(P.status, CNB_FLAG_LIST_OVERFLOW);
-    if (P.stats && lane == 0) {
-        // n_inter counts list entries per warp (each applied to 32 lanes)
-        atomicAdd(P.stats, n_inter);
-    }
     if (P.stats) {
         for (int o = 16; o > 0; o >>= 1) n_tests += __shfl_xor_sync(0xffffffffu, n_tests, o);
         if (lane == 0) atomicAdd(P.stats + 1, n_tests);
     }
+    if (lane == 0) atomicMax(P.ws + 2, max_top);
 }
 
-// Node table for the grouped traversal from the reference-layout tree.
+// Traversal node table from the reference-layout tree: 32-byte records
+// (com, mass | x-extent, 3-D extent, children) and the boxes (min | max).
 __global__ void __launch_bounds__(256) k_pack_nodes(const float *__restrict__ n_mass,
                                                     const float *__restrict__ n_com,
                                                     const float *__restrict__ n_min,
                                                     const float *__restrict__ n_max,
                                                     const int2 *__restrict__ children,
-                                                    float4 *__restrict__ A, float4 *__restrict__ B,
-                                                    float4 *__restrict__ C, int64_t m) {
+                                                    float4 *__restrict__ rec,
+                                                    float4 *__restrict__ aabb, int64_t m) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < m;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int2 ch = children[i];
-        A[i] = make_float4(n_com[3 * i], n_com[3 * i + 1], n_com[3 * i + 2], n_mass[i]);
-        B[i] = make_float4(n_min[3 * i], n_min[3 * i + 1], n_min[3 * i + 2], __int_as_float(ch.x));
-        C[i] = make_float4(n_max[3 * i], n_max[3 * i + 1], n_max[3 * i + 2], __int_as_float(ch.y));
+        const float lx = n_min[3 * i], ly = n_min[3 * i + 1], lz = n_min[3 * i + 2];
+        const float hx = n_max[3 * i], hy = n_max[3 * i + 1], hz = n_max[3 * i + 2];
+        const float sx = hx - lx;  // physics_kernels.py:131 (before the clamp)
+        const float l3 = fmaxf(sx, fmaxf(hy - ly, hz - lz));
+        rec[2 * i] = make_float4(n_com[3 * i], n_com[3 * i + 1], n_com[3 * i + 2], n_mass[i]);
+        rec[2 * i + 1] = make_float4(sx, l3, __int_as_float(ch.x), __int_as_float(ch.y));
+        aabb[2 * i] = make_float4(lx, ly, lz, 0.f);
+        aabb[2 * i + 1] = make_float4(hx, hy, hz, 0.f);
     }
 }
 
@@ -241,47 +312,95 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
         return CNB_E_INVALID_ARG;
     if ((reinterpret_cast<uintptr_t>(node_table) & 15) || (reinterpret_cast<uintptr_t>(children) & 7))
         return CNB_E_INVALID_ARG;
-    float4 *A = reinterpret_cast<float4 *>(node_table);
+    float4 *rec = reinterpret_cast<float4 *>(node_table);
     k_pack_nodes<<<grid_for(n_nodes, 256), 256, 0, as_stream(stream)>>>(
-        n_mass, n_com, n_min, n_max, reinterpret_cast<const int2 *>(children), A, A + n_nodes,
-        A + 2 * n_nodes, n_nodes);
+        n_mass, n_com, n_min, n_max, reinterpret_cast<const int2 *>(children), rec,
+        rec + 2 * n_nodes, n_nodes);
     return launch_status();
 }
 
-extern "C" int cnb_forces_grouped(const float *px, const float *py, const float *pz,
-                                  const float *node_table, float *force, int64_t n, double theta,
-                                  const float *theta_per_group, int mac, double G, double soft,
-                                  double box, unsigned long long *stats, int32_t *status,
-                                  void *stream) {
+static int launch_grouped(GroupedParams &P, int bodies_per_lane, cudaStream_t st) {
+    // persistent grid: the work counter hands out buckets
+    CNB_CUDA(cudaMemsetAsync(P.ws + 1, 0, 2 * sizeof(int32_t), st));
+    int per_sm = 0;
+    if (bodies_per_lane == 1) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<1>, kGWarps * 32, 0);
+        k_forces_grouped<1><<<kSMs * (per_sm > 0 ? per_sm : 1), kGWarps * 32, 0, st>>>(P);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<2>, kGWarps * 32, 0);
+        k_forces_grouped<2><<<kSMs * (per_sm > 0 ? per_sm : 1), kGWarps * 32, 0, st>>>(P);
+    }
+    return launch_status();
+}
+
+static int grouped_common(GroupedParams &P, const float *px, const float *py, const float *pz,
+                          const float *node_table, int32_t *workspace, float *force, int64_t n,
+                          const float *theta_per_bucket, int mac, int bodies_per_lane, double G,
+                          unsigned long long *stats, int32_t *status) {
     if (n < 0 || (mac != CNB_MAC_REF_X && mac != CNB_MAC_PERIODIC)) return CNB_E_INVALID_ARG;
+    if (bodies_per_lane != 1 && bodies_per_lane != 2) return CNB_E_INVALID_ARG;
     if (n == 0) return CNB_OK;
-    if (!px || !py || !pz || !node_table || !force) return CNB_E_INVALID_ARG;
-    if (reinterpret_cast<uintptr_t>(node_table) & 15) return CNB_E_INVALID_ARG;
+    if (!px || !py || !pz || !node_table || !force || !workspace) return CNB_E_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(node_table) & 15) || (reinterpret_cast<uintptr_t>(workspace) & 15))
+        return CNB_E_INVALID_ARG;
     if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
     const int64_t m = 2 * n - 1;
-    GroupedParams P;
+    P = GroupedParams{};
     P.px = px;
     P.py = py;
     P.pz = pz;
-    P.nA = reinterpret_cast<const float4 *>(node_table);
-    P.nB = P.nA + m;
-    P.nC = P.nA + 2 * m;
+    P.rec = reinterpret_cast<const float4 *>(node_table);
+    P.aabb = P.rec + 2 * m;
     P.force = force;
-    P.theta_per_group = theta_per_group;
-    P.theta = (float)theta;
+    P.ws = workspace;
+    P.buckets = reinterpret_cast<const int2 *>(workspace + 4);
+    P.theta_per_bucket = theta_per_bucket;
     P.G = (float)G;
-    P.soft2 = (float)(soft * soft);
-    P.box = (float)box;
+    P.box = 1.0f;
     P.mac = mac;
     P.n = n;
     P.m_nodes = m;
     P.root = n > 1 ? (int32_t)n : 0;
-    P.n_groups = (n + 31) / 32;
     P.stats = stats;
     P.status = status;
-    const int64_t blocks_needed = (P.n_groups + kGWarps - 1) / kGWarps;
-    const int64_t cap = 148LL * 64;
-    const int grid = (int)(blocks_needed < cap ? blocks_needed : cap);
-    k_forces_grouped<<<grid, kGWarps * 32, 0, as_stream(stream)>>>(P);
-    return launch_status();
+    return CNB_OK;
+}
+
+extern "C" int cnb_forces_grouped(const float *px, const float *py, const float *pz,
+                                  const float *node_table, int32_t *workspace, float *force,
+                                  int64_t n, double theta, const float *theta_per_bucket,
+                                  int mac, int bodies_per_lane, double G, double soft, double box,
+                                  double slab_mass, unsigned long long *stats, int32_t *status,
+                                  void *stream) {
+    GroupedParams P;
+    CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket, mac,
+                           bodies_per_lane, G, stats, status));
+    if (n == 0) return CNB_OK;
+    P.theta = (float)theta;
+    P.soft2 = (float)(soft * soft);
+    P.box = (float)box;
+    P.slab_mass = (float)slab_mass;
+    return launch_grouped(P, bodies_per_lane, as_stream(stream));
+}
+
+extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,
+                                        const float *node_table, int32_t *workspace, float *force,
+                                        int64_t n, const uint64_t *codes, int box_bits,
+                                        const int32_t *box_roots, const float *box_params,
+                                        const float *theta_per_bucket, int mac,
+                                        int bodies_per_lane, double G,
+                                        unsigned long long *stats, int32_t *status,
+                                        void *stream) {
+    GroupedParams P;
+    CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket, mac,
+                           bodies_per_lane, G, stats, status));
+    if (n == 0) return CNB_OK;
+    if (!codes || !box_roots || !box_params || box_bits < 0 || box_bits > 30)
+        return CNB_E_INVALID_ARG;
+    if (reinterpret_cast<uintptr_t>(box_params) & 15) return CNB_E_INVALID_ARG;
+    P.codes = codes;
+    P.box_shift = 3 * ((63 - box_bits) / 3);
+    P.box_roots = box_roots;
+    P.box_params = reinterpret_cast<const float4 *>(box_params);
+    return launch_grouped(P, bodies_per_lane, as_stream(stream));
 }

@@ -3,9 +3,11 @@
 //
 // One pass per 8-bit digit, reduce-then-scan (no inter-block waiting):
 //   k_digit_count   per-tile digit counts (shared-memory histograms)
-//   k_count_scan    exclusive scan of the counts, digit-major, tile-minor
+//   k_scan_rows     exclusive scan of each digit's tile counts (one block
+//                   per digit) and the digit totals
 //   k_scatter       stable in-tile ranks (warp __match_any_sync + per-warp
-//                   digit counters) and the scatter to global positions
+//                   digit counters), the tile reordered by digit in shared
+//                   memory, then coalesced runs written to global positions
 // A 4096-key tile per 256-thread block keeps one pass at 8 B read for the
 // count, 12 B read + 12 B written for the scatter, per key.
 #include <new>
@@ -40,21 +42,23 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_count(const uint64_t *__
     }
 }
 
-// Single-block exclusive scan over `len` counts (in place).
-__global__ void __launch_bounds__(1024) k_count_scan(uint32_t *__restrict__ hist, int64_t len) {
-    __shared__ uint32_t warp_sums[32];
+// Exclusive scan of one digit's row of tile counts (in place), one block per
+// digit; the row total goes to totals[digit].
+__global__ void __launch_bounds__(256) k_scan_rows(uint32_t *__restrict__ hist, int64_t tiles,
+                                                   uint32_t *__restrict__ totals) {
+    __shared__ uint32_t warp_sums[8];
     __shared__ uint32_t carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t *row = hist + (int64_t)blockIdx.x * tiles;
     if (threadIdx.x == 0) carry = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t chunk = 1024LL * 8;
-    for (int64_t base = 0; base < len; base += chunk) {
-        uint32_t v[8];
+    for (int64_t base = 0; base < tiles; base += 256 * 4) {
+        uint32_t v[4];
         uint32_t local = 0;
-        int64_t b0 = base + (int64_t)threadIdx.x * 8;
+        const int64_t b0 = base + (int64_t)threadIdx.x * 4;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            v[k] = (b0 + k < len) ? hist[b0 + k] : 0u;
+        for (int k = 0; k < 4; ++k) {
+            v[k] = (b0 + k < tiles) ? row[b0 + k] : 0u;
             local += v[k];
         }
         uint32_t incl = local;
@@ -65,29 +69,49 @@ __global__ void __launch_bounds__(1024) k_count_scan(uint32_t *__restrict__ hist
         }
         if (lane == 31) warp_sums[warp] = incl;
         __syncthreads();
-        if (warp == 0) {
-            uint32_t ws = warp_sums[lane];
-            uint32_t wi = ws;
+        uint32_t wbase = 0, total = 0;
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                uint32_t t = __shfl_up_sync(0xffffffffu, wi, o);
-                if (lane >= o) wi += t;
-            }
-            warp_sums[lane] = wi - ws;
+        for (int w = 0; w < 8; ++w) {
+            wbase += (w < warp) ? warp_sums[w] : 0u;
+            total += warp_sums[w];
         }
-        __syncthreads();
-        uint32_t run = carry + warp_sums[warp] + (incl - local);
+        uint32_t run = carry + wbase + (incl - local);
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (b0 + k < len) hist[b0 + k] = run;
+        for (int k = 0; k < 4; ++k) {
+            if (b0 + k < tiles) row[b0 + k] = run;
             run += v[k];
         }
         __syncthreads();
-        if (threadIdx.x == 1023) carry = run;
+        if (threadIdx.x == 0) carry += total;
         __syncthreads();
     }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
 }
 
+// Exclusive block scan of 256 values held one per thread (blockDim == 256).
+__device__ __forceinline__ uint32_t block_exscan256(uint32_t v, uint32_t *warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) wbase += (w < warp) ? warp_sums[w] : 0u;
+    __syncthreads();
+    return wbase + incl - v;
+}
+
+constexpr int kScatterSmem = kSortTile * (sizeof(uint64_t) + sizeof(uint32_t));
+
+// One pass of the LSD sort over a 4096-key tile: stable ranks within the
+// tile (warp __match_any_sync + per-warp digit counters), the tile sorted by
+// digit in shared memory, then written out in runs so that consecutive
+// threads store consecutive global positions.
 template <bool IDENTITY_IN>
 __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t *__restrict__ kin,
                                                           const uint32_t *__restrict__ vin,
@@ -95,24 +119,36 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t *__rest
                                                           uint32_t *__restrict__ vout,
                                                           int64_t n, int shift,
                                                           const uint32_t *__restrict__ offs,
+                                                          const uint32_t *__restrict__ totals,
                                                           int64_t tiles) {
+    static_assert(kSortThreads == 256, "block scans assume 256 threads");
     constexpr int W = kSortThreads / 32;
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t *skey = reinterpret_cast<uint64_t *>(smem);
+    uint32_t *sval = reinterpret_cast<uint32_t *>(smem + kSortTile * sizeof(uint64_t));
     __shared__ uint32_t wcnt[W][257];
     __shared__ uint32_t gbase[256];
+    __shared__ uint32_t tstart[256];
+    __shared__ uint32_t wsum[8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < W * 257; i += kSortThreads) (&wcnt[0][0])[i] = 0;
-    for (int d = threadIdx.x; d < 256; d += kSortThreads)
-        gbase[d] = offs[(int64_t)d * tiles + blockIdx.x];
+    {
+        // global start of each digit: digits before it + this digit in earlier tiles
+        const int d = threadIdx.x;
+        const uint32_t base = block_exscan256(totals[d], wsum);
+        gbase[d] = base + offs[(int64_t)d * tiles + blockIdx.x];
+    }
     __syncthreads();
 
     const uint32_t lt_mask = (1u << lane) - 1u;
-    const int64_t wbase = (int64_t)blockIdx.x * kSortTile + (int64_t)warp * 32 * kSortItems;
+    const int64_t tbase = (int64_t)blockIdx.x * kSortTile;
+    const int64_t wbase = tbase + (int64_t)warp * 32 * kSortItems;
     uint64_t key[kSortItems];
     uint32_t val[kSortItems];
     uint32_t rank[kSortItems];
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        int64_t e = wbase + r * 32 + lane;
+        const int64_t e = wbase + r * 32 + lane;
         uint32_t d = 256;  // sentinel for lanes past the end
         if (e < n) {
             key[r] = kin[e];
@@ -122,34 +158,45 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t *__rest
             key[r] = 0;
             val[r] = 0;
         }
-        uint32_t peers = __match_any_sync(0xffffffffu, d);
-        uint32_t before = wcnt[warp][d];
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = wcnt[warp][d];
         __syncwarp();
         if ((peers & lt_mask) == 0) wcnt[warp][d] = before + __popc(peers);
         __syncwarp();
         rank[r] = before + __popc(peers & lt_mask);
     }
     __syncthreads();
-    // exclusive prefix over warps, per digit
-    for (int d = threadIdx.x; d < 256; d += kSortThreads) {
+    {
+        // per digit: exclusive prefix over warps, then the digit's start in the tile
+        const int d = threadIdx.x;
         uint32_t run = 0;
 #pragma unroll
         for (int w = 0; w < W; ++w) {
-            uint32_t c = wcnt[w][d];
+            const uint32_t c = wcnt[w][d];
             wcnt[w][d] = run;
             run += c;
         }
+        tstart[d] = block_exscan256(run, wsum);
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < kSortItems; ++r) {
-        int64_t e = wbase + r * 32 + lane;
+        const int64_t e = wbase + r * 32 + lane;
         if (e < n) {
-            uint32_t d = (uint32_t)(key[r] >> shift) & 255u;
-            int64_t pos = (int64_t)gbase[d] + wcnt[warp][d] + rank[r];
-            kout[pos] = key[r];
-            vout[pos] = val[r];
+            const uint32_t d = (uint32_t)(key[r] >> shift) & 255u;
+            const uint32_t lp = tstart[d] + wcnt[warp][d] + rank[r];
+            skey[lp] = key[r];
+            sval[lp] = val[r];
         }
+    }
+    __syncthreads();
+    const int tile_n = (int)min((int64_t)kSortTile, n - tbase);
+    for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
+        const uint64_t k = skey[j];
+        const uint32_t d = (uint32_t)(k >> shift) & 255u;
+        const int64_t pos = (int64_t)gbase[d] + (j - tstart[d]);
+        kout[pos] = k;
+        vout[pos] = sval[j];
     }
 }
 
@@ -177,6 +224,11 @@ int sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
     if (passes < 1) passes = 1;
     if (passes == 1 && keys_in == keys_out) passes = 2;
     const int64_t tiles = (n + kSortTile - 1) / kSortTile;
+    // the scatter's staging tile is above the 48 KB default (cheap host call)
+    CNB_CUDA(cudaFuncSetAttribute(k_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kScatterSmem));
+    CNB_CUDA(cudaFuncSetAttribute(k_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kScatterSmem));
     const uint64_t *ks = keys_in;
     const uint32_t *vs = idx_in;
     for (int p = 0; p < passes; ++p) {
@@ -184,18 +236,18 @@ int sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
         const bool last = (p == passes - 1);
         uint64_t *kd = last ? keys_out : ctx->keys_tmp[p & 1];
         uint32_t *vd = last ? perm_out : ctx->vals_tmp[p & 1];
+        uint32_t *totals = ctx->tile_hist + 256 * tiles;
         k_digit_count<<<(unsigned)tiles, kSortThreads, 0, st>>>(ks, n, shift, ctx->tile_hist,
                                                                tiles);
         CNB_TRY(launch_status());
-        k_count_scan<<<1, 1024, 0, st>>>(ctx->tile_hist, 256 * tiles);
+        k_scan_rows<<<256, 256, 0, st>>>(ctx->tile_hist, tiles, totals);
         CNB_TRY(launch_status());
         if (vs == nullptr)
-            k_scatter<true><<<(unsigned)tiles, kSortThreads, 0, st>>>(ks, nullptr, kd, vd, n,
-                                                                      shift, ctx->tile_hist,
-                                                                      tiles);
+            k_scatter<true><<<(unsigned)tiles, kSortThreads, kScatterSmem, st>>>(
+                ks, nullptr, kd, vd, n, shift, ctx->tile_hist, totals, tiles);
         else
-            k_scatter<false><<<(unsigned)tiles, kSortThreads, 0, st>>>(ks, vs, kd, vd, n, shift,
-                                                                       ctx->tile_hist, tiles);
+            k_scatter<false><<<(unsigned)tiles, kSortThreads, kScatterSmem, st>>>(
+                ks, vs, kd, vd, n, shift, ctx->tile_hist, totals, tiles);
         CNB_TRY(launch_status());
         ks = kd;
         vs = vd;
@@ -238,7 +290,7 @@ extern "C" int cnb_ctx_create(int64_t n_max, cnb_ctx **out) {
         e = cudaMalloc(&c->keys_tmp[k], sizeof(uint64_t) * nn);
         if (e == cudaSuccess) e = cudaMalloc(&c->vals_tmp[k], sizeof(uint32_t) * nn);
     }
-    if (e == cudaSuccess) e = cudaMalloc(&c->tile_hist, sizeof(uint32_t) * 256 * c->tiles_max);
+    if (e == cudaSuccess) e = cudaMalloc(&c->tile_hist, sizeof(uint32_t) * 256 * (c->tiles_max + 1));
     if (e != cudaSuccess) {
         cnb_ctx_destroy(c);
         cnb::record_cuda_error(e);

@@ -31,7 +31,7 @@ constexpr int64_t kMaxKeys = CNB_NOALLOC_MAX_KEYS;
 constexpr int64_t kMaxTiles = (kMaxKeys + kSortTile - 1) / kSortTile;
 constexpr size_t kKeyBytes = sizeof(uint64_t) * kMaxKeys;
 constexpr size_t kValBytes = sizeof(uint32_t) * kMaxKeys;
-constexpr size_t kHistBytes = sizeof(uint32_t) * 256 * kMaxTiles;
+constexpr size_t kHistBytes = sizeof(uint32_t) * 256 * (kMaxTiles + 1);  // counts + digit totals
 constexpr size_t kScratchBytes = 2 * kKeyBytes + 2 * kValBytes + kHistBytes;
 
 constexpr int kMaxDevices = 64;

@@ -35,7 +35,8 @@ __device__ __forceinline__ int delta_fn(const uint64_t *__restrict__ codes, uint
 // tree_kernels.py:60-129 build_tree, one thread per split i < n-1.
 __global__ void __launch_bounds__(256) k_build_tree(const uint64_t *__restrict__ codes,
                                                     int32_t *__restrict__ children,
-                                                    int32_t *__restrict__ parents, int64_t n) {
+                                                    int32_t *__restrict__ parents, int64_t n,
+                                                    int2 *__restrict__ ranges) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1;
          i += (int64_t)gridDim.x * blockDim.x) {
         const uint64_t ki = __ldg(codes + i);
@@ -66,6 +67,49 @@ __global__ void __launch_bounds__(256) k_build_tree(const uint64_t *__restrict__
         children[2 * idx + 1] = c1;
         parents[c0] = (int32_t)idx;
         parents[c1] = (int32_t)idx;
+        if (ranges) ranges[i] = make_int2((int)lo, (int)hi);
+    }
+}
+
+// Bucket table for the grouped traversal: the maximal subtrees holding at
+// most `max_size` bodies (a node qualifies when it is small enough and its
+// parent is not).  Such buckets are contiguous in the sorted order and
+// spatially compact (a radix-tree node covers one key prefix).  Appended in
+// any order; ws[0] receives the count, ws[1] (the traversal's work counter)
+// is reset.
+__global__ void __launch_bounds__(256) k_make_buckets(const int2 *__restrict__ ranges,
+                                                      const int32_t *__restrict__ parents,
+                                                      int64_t n, int max_size,
+                                                      int32_t *__restrict__ ws,
+                                                      int2 *__restrict__ buckets,
+                                                      const uint64_t *__restrict__ codes,
+                                                      int box_shift) {
+    const int64_t m = 2 * n - 1;
+    for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < m;
+         v += (int64_t)gridDim.x * blockDim.x) {
+        int lo, size;
+        if (v < n) {
+            lo = (int)v;
+            size = 1;
+        } else {
+            const int2 r = ranges[v - n];
+            lo = r.x;
+            size = r.y - r.x + 1;
+        }
+        if (size > max_size) continue;
+        // with several boxes in the tree a bucket never spans two boxes
+        if (codes && (codes[lo] >> box_shift) != (codes[lo + size - 1] >> box_shift)) continue;
+        const int32_t p = parents[v];
+        bool top = (p < 0);
+        if (!top) {
+            const int2 pr = ranges[p - n];
+            top = (pr.y - pr.x + 1) > max_size ||
+                  (codes && (codes[pr.x] >> box_shift) != (codes[pr.y] >> box_shift));
+        }
+        if (top) {
+            const int slot = atomicAdd(ws, 1);
+            buckets[slot] = make_int2(lo, size);
+        }
     }
 }
 
@@ -331,8 +375,55 @@ extern "C" int cnb_build_tree(const uint64_t *codes, int32_t *children, int32_t 
     if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
     if (n < 2) return CNB_OK;
     k_build_tree<<<grid_for(n - 1, 256), 256, 0, as_stream(stream)>>>(codes, children, parents,
-                                                                       n);
+                                                                       n, nullptr);
     return launch_status();
+}
+
+extern "C" int cnb_build_tree_ranges(const uint64_t *codes, int32_t *children, int32_t *parents,
+                                     int32_t *ranges, int64_t n, void *stream) {
+    if (n < 0 || (n > 1 && (!codes || !children || !parents || !ranges))) return CNB_E_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(ranges) & 7) != 0) return CNB_E_INVALID_ARG;
+    if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
+    if (n < 2) return CNB_OK;
+    k_build_tree<<<grid_for(n - 1, 256), 256, 0, as_stream(stream)>>>(
+        codes, children, parents, n, reinterpret_cast<int2 *>(ranges));
+    return launch_status();
+}
+
+static int make_buckets(const int32_t *ranges, const int32_t *parents, const uint64_t *codes,
+                        int box_shift, int64_t n, int max_size, int32_t *workspace,
+                        void *stream) {
+    if (n < 0 || max_size < 1 || !workspace) return CNB_E_INVALID_ARG;
+    if (n > 1 && (!ranges || !parents)) return CNB_E_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return CNB_E_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    CNB_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+    int2 *buckets = reinterpret_cast<int2 *>(workspace + 4);
+    if (n == 0) return CNB_OK;
+    if (n == 1) {
+        const int32_t one[4] = {1, 0, 0, 0};
+        const int32_t b[2] = {0, 1};
+        CNB_CUDA(cudaMemcpyAsync(workspace, one, sizeof(one), cudaMemcpyHostToDevice, st));
+        CNB_CUDA(cudaMemcpyAsync(buckets, b, sizeof(b), cudaMemcpyHostToDevice, st));
+        return CNB_OK;
+    }
+    k_make_buckets<<<grid_for(2 * n - 1, 256), 256, 0, st>>>(
+        reinterpret_cast<const int2 *>(ranges), parents, n, max_size, workspace, buckets, codes,
+        box_shift);
+    return launch_status();
+}
+
+extern "C" int cnb_make_buckets(const int32_t *ranges, const int32_t *parents, int64_t n,
+                                int max_size, int32_t *workspace, void *stream) {
+    return make_buckets(ranges, parents, nullptr, 0, n, max_size, workspace, stream);
+}
+
+extern "C" int cnb_make_buckets_boxes(const int32_t *ranges, const int32_t *parents,
+                                      const uint64_t *codes, int box_bits, int64_t n,
+                                      int max_size, int32_t *workspace, void *stream) {
+    if (!codes || box_bits < 0 || box_bits > 30) return CNB_E_INVALID_ARG;
+    return make_buckets(ranges, parents, codes, 3 * ((63 - box_bits) / 3), n, max_size,
+                        workspace, stream);
 }
 
 static int upward_impl(const float *px, const float *py, const float *pz, const float *mass,

@@ -165,23 +165,81 @@ int cnb_integrate(float *px, float *py, float *pz, float *vx, float *vy, float *
 int cnb_render_density(const float *px, const float *py, const float *pz, float *grid,
                        const float *mvp, int64_t n, int width, int height, void *stream);
 
-/* Node table for cnb_forces_grouped: three float4 arrays of n_nodes entries,
- * back to back: (com, mass), (min, child0 bits), (max, child1 bits), built
- * from the reference-layout tree (normalised n_com).  16-byte aligned. */
+/* src/kernels/tree_kernels.py:60-129 build_tree plus the index range
+ * [lo, hi] of every internal node's bodies: ranges is int32 [N-1, 2]
+ * (internal node N+i -> ranges[i]), 8-byte aligned.  Same children/parents
+ * as cnb_build_tree. */
+int cnb_build_tree_ranges(const uint64_t *codes, int32_t *children, int32_t *parents,
+                          int32_t *ranges, int64_t n, void *stream);
+
+/* Bucket table for cnb_forces_grouped (no reference counterpart): the
+ * maximal subtrees holding at most max_size bodies.  workspace (device,
+ * 16-byte aligned) is int32 [4 + 2N]: [0] bucket count, [1] work counter,
+ * [2] deepest node stack seen by the traversal, [3] unused, then one
+ * (first body, count) pair per bucket. */
+int cnb_make_buckets(const int32_t *ranges, const int32_t *parents, int64_t n, int max_size,
+                     int32_t *workspace, void *stream);
+
+/* cnb_make_buckets for several boxes in one tree (keys of
+ * cnb_compute_codes_boxes): no bucket spans two boxes. */
+int cnb_make_buckets_boxes(const int32_t *ranges, const int32_t *parents, const uint64_t *codes,
+                           int box_bits, int64_t n, int max_size, int32_t *workspace,
+                           void *stream);
+
+/* Node table for cnb_forces_grouped: float32 [4, n_nodes, 4], 16-byte
+ * aligned: 32-byte records (com x, y, z, mass | x-extent, 3-D extent,
+ * child0 bits, child1 bits) for every node, then the boxes (min | max).
+ * Built from the reference-layout tree (normalised n_com). */
 int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
                    const float *n_max, const int32_t *children, float *node_table,
                    int64_t n_nodes, void *stream);
 
-/* The B200 form of src/kernels/physics_kernels.py:14-153: one warp per bucket
- * of 32 Morton-consecutive bodies, shared-memory node stack and interaction
- * list, float32 with rsqrt and per-pair minimum image.  theta_per_group
- * (device, ceil(n/32) floats, may be NULL) overrides theta per bucket.  mac:
- * CNB_MAC_REF_X or CNB_MAC_PERIODIC.  stats (device, 2 x uint64, may be
- * NULL) accumulates [interactions, node tests]. */
+/* The B200 form of src/kernels/physics_kernels.py:14-153: one warp per
+ * bucket of cnb_make_buckets (at most 32 * bodies_per_lane bodies, buckets
+ * handed out by an atomic work counter), shared-memory node stack and
+ * interaction list, float32 with rsqrt, the minimum image per pair only
+ * where a bucket's bodies can see different images.  theta_per_bucket
+ * (device float per bucket slot, may be NULL) overrides theta.  mac:
+ * CNB_MAC_REF_X or CNB_MAC_PERIODIC.  bodies_per_lane: 1 or 2.  slab_mass
+ * (CNB_MAC_PERIODIC only): nodes whose image differs between a bucket's
+ * bodies are opened unless their mass is at most slab_mass, in which case
+ * they are applied with the per-pair minimum image of their CoM (0 = exact
+ * minimum-image semantics).  stats (device, 2 x uint64, may be NULL)
+ * accumulates [body-node interactions, node tests]. */
 int cnb_forces_grouped(const float *px, const float *py, const float *pz,
-                       const float *node_table, float *force, int64_t n, double theta,
-                       const float *theta_per_group, int mac, double G, double soft, double box,
+                       const float *node_table, int32_t *workspace, float *force, int64_t n,
+                       double theta, const float *theta_per_bucket, int mac, int bodies_per_lane,
+                       double G, double soft, double box, double slab_mass,
                        unsigned long long *stats, int32_t *status, void *stream);
+
+/* ---- many independent boxes in one launch (no reference counterpart) ----
+ * Keys carry the box id in their top bits: key = box << 3L | morton_L(x,y,z),
+ * L = (63 - box_bits) / 3 bits per axis, coordinates in each box's own unit
+ * cube.  One sort and one Karras build then make every box one subtree. */
+int cnb_compute_codes_boxes(const float *x, const float *y, const float *z, const int32_t *box,
+                            uint64_t *codes, int64_t n, int box_bits, void *stream);
+
+/* Subtree root of every box (int32 [n_boxes], -1 for an empty box) from the
+ * sorted box keys and the tree of cnb_build_tree_ranges. */
+int cnb_box_roots(const int32_t *ranges, const int32_t *parents, const uint64_t *codes,
+                  int box_bits, int64_t n, int n_boxes, int32_t *roots, void *stream);
+
+/* cnb_forces_grouped over many boxes: every bucket walks its own box's
+ * subtree with its box's (theta, softening, slab mass, unused) from
+ * box_params (float32 [n_boxes, 4], 16-byte aligned); theta_per_bucket, if
+ * given, overrides theta.  Each box is periodic on its own unit cube. */
+int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,
+                             const float *node_table, int32_t *workspace, float *force, int64_t n,
+                             const uint64_t *codes, int box_bits, const int32_t *box_roots,
+                             const float *box_params, const float *theta_per_bucket, int mac,
+                             int bodies_per_lane, double G, unsigned long long *stats,
+                             int32_t *status, void *stream);
+
+/* physics_kernels.py:155-203 integrate with per-box (a, H, dt): box_aHdt is
+ * float64 [n_boxes, 3] on the device, so a captured step can advance it. */
+int cnb_integrate_boxes(float *px, float *py, float *pz, float *vx, float *vy, float *vz,
+                        const float *force, const uint64_t *codes, int box_bits, int64_t n,
+                        const double *box_aHdt, void *stream);
 
 /* Float64 minimum-image direct sum (the force law of
  * src/kernels/physics_kernels.py:118-141 over every pair) for the bodies

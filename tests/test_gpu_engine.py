@@ -232,4 +232,5 @@ def test_bad_arguments_raise():
         build_tree[1, 256](codes.to(torch.int64), child, torch.zeros(19, dtype=torch.int32, device="cuda"))
     from cnb import _lib
     with pytest.raises(CnbError):
-        _lib.call("cnb_forces_grouped", 1, 1, 1, 1, 1, 10, 0.5, None, 9, 1.0, 0.1, 1.0, None, None, None)
+        _lib.call("cnb_forces_grouped", 16, 16, 16, 16, 16, 16, 10, 0.5, None, 9, 1, 1.0, 0.1, 1.0,
+                  0.0, None, None, None)

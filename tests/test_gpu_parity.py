@@ -423,22 +423,37 @@ def test_direct_sum_gpu_matches_oracle():
     np.testing.assert_allclose(got, want, rtol=0, atol=1e-11 * np.abs(want).max())
 
 
-def grouped(pos, nodes, theta, soft, mac, tpg=None):
+def grouped(pos, codes, mass, theta, soft, mac, tpg=None, bpl=1, want_ws=False, slab=0.0):
+    """Tree (with node ranges), node table, buckets and the grouped traversal."""
     n = pos[0].size
     m = 2 * n - 1
+    K = dev(codes)
+    ch = torch.full((m, 2), -1, dtype=torch.int32, device="cuda")
+    par = torch.full((m,), -1, dtype=torch.int32, device="cuda")
+    rng_ = torch.zeros((max(n - 1, 1), 2), dtype=torch.int32, device="cuda")
+    lib().call("cnb_build_tree_ranges", K.data_ptr(), ch.data_ptr(), par.data_ptr(), rng_.data_ptr(),
+               n, stream())
+    cnt = torch.zeros(m, dtype=torch.int32, device="cuda")
     P = [dev(a) for a in pos]
-    table = torch.empty((3, m, 4), dtype=torch.float32, device="cuda")
-    ch = nodes[0]
-    lib().call("cnb_pack_nodes", *(t.data_ptr() for t in nodes[1]), ch.data_ptr(),
-               table.data_ptr(), m, stream())
+    M = dev(mass)
+    nodes = [torch.zeros(m, device="cuda"), torch.zeros((m, 3), device="cuda"),
+             torch.zeros((m, 3), device="cuda"), torch.zeros((m, 3), device="cuda")]
+    lib().call("cnb_upward", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(), par.data_ptr(),
+               *(t.data_ptr() for t in nodes), None, cnt.data_ptr(), n, 0, None, None, stream())
+    table = torch.empty((4, m, 4), dtype=torch.float32, device="cuda")
+    lib().call("cnb_pack_nodes", *(t.data_ptr() for t in nodes), ch.data_ptr(), table.data_ptr(), m,
+               stream())
+    ws = torch.zeros(4 + 2 * n, dtype=torch.int32, device="cuda")
+    lib().call("cnb_make_buckets", rng_.data_ptr(), par.data_ptr(), n, 32 * bpl, ws.data_ptr(), stream())
     F = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
     stats = torch.zeros(2, dtype=torch.int64, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     T = dev(tpg.astype(np.float32)) if tpg is not None else None
-    lib().call("cnb_forces_grouped", *(p.data_ptr() for p in P), table.data_ptr(), F.data_ptr(), n,
-               theta, T.data_ptr() if T is not None else None, mac, 1.0, soft, 1.0,
-               stats.data_ptr(), status.data_ptr(), stream())
-    return host(F), host(stats), int(host(status)[0])
+    lib().call("cnb_forces_grouped", *(p.data_ptr() for p in P), table.data_ptr(), ws.data_ptr(),
+               F.data_ptr(), n, theta, T.data_ptr() if T is not None else None, mac, bpl, 1.0, soft,
+               1.0, slab, stats.data_ptr(), status.data_ptr(), stream())
+    out = (host(F), host(stats), int(host(status)[0]))
+    return out + (host(ws),) if want_ws else out
 
 
 def rel_err(a, ref):
@@ -446,22 +461,39 @@ def rel_err(a, ref):
 
 
 @pytest.mark.parametrize("mac", [0, 1])
-def test_grouped_theta_zero_is_direct_sum(mac):
+@pytest.mark.parametrize("bpl", [1, 2])
+def test_grouped_theta_zero_is_direct_sum(mac, bpl):
     # with theta -> 0 every node is opened: the grouped kernel becomes the
     # float32 minimum-image direct sum
     pos, _, codes = sorted_case(16, 0, 1)
     n = codes.size
     mass = np.full(n, 1.0 / n, np.float32)
-    ch, root, nodes, hn = tree_on_gpu(pos, mass, codes)
     soft = 0.5 / 16
-    got, stats, st = grouped(pos, (ch, nodes), 1e-6, soft, mac)
+    got, stats, st = grouped(pos, codes, mass, 1e-6, soft, mac, bpl=bpl)
     assert st == 0
     t = np.arange(0, n, 7)
     want = direct_gpu(pos, mass, t, soft)
     e = rel_err(got[t].astype(np.float64), want)
     assert np.median(e) < 1e-4 and e.max() < 5e-3
-    # every body interacted with all n bodies (leaves), once per warp entry
-    assert stats[0] == ((n + 31) // 32) * n
+    # every body met every body (leaves) exactly once
+    assert stats[0] == n * n
+
+
+@pytest.mark.parametrize("bpl", [1, 2])
+def test_buckets_partition_the_bodies(bpl):
+    pos, _, codes = sorted_case(32, 1, 1)
+    n = codes.size
+    mass = np.full(n, 1.0 / n, np.float32)
+    _, _, st, ws = grouped(pos, codes, mass, 0.5, 0.01, 0, bpl=bpl, want_ws=True)
+    assert st == 0
+    nb = ws[0]
+    b = ws[4:4 + 2 * nb].reshape(nb, 2)
+    assert b[:, 1].max() <= 32 * bpl and b[:, 1].min() >= 1
+    order = np.argsort(b[:, 0])
+    starts, counts = b[order, 0], b[order, 1]
+    np.testing.assert_array_equal(starts[1:], (starts + counts)[:-1])
+    assert starts[0] == 0 and starts[-1] + counts[-1] == n
+    assert 0 < ws[2] <= 2048   # deepest node stack
 
 
 def test_grouped_ref_mac_accuracy_vs_reference_traversal():
@@ -472,7 +504,7 @@ def test_grouped_ref_mac_accuracy_vs_reference_traversal():
     mass = np.full(n, 1.0 / n, np.float32)
     ch, root, nodes, hn = tree_on_gpu(pos, mass, codes)
     soft = 0.5 / 32
-    g, _, st = grouped(pos, (ch, nodes), 0.5, soft, 0)
+    g, _, st = grouped(pos, codes, mass, 0.5, soft, 0)
     assert st == 0
     r, _ = gpu_forces_ref(pos, ch, root, nodes, 0.5, soft, 1)
     t = np.random.default_rng(1).choice(n, 1024, replace=False)
@@ -485,13 +517,12 @@ def test_grouped_periodic_mac_accuracy():
     pos, _, codes = sorted_case(32, 0, 1)
     n = codes.size
     mass = np.full(n, 1.0 / n, np.float32)
-    ch, root, nodes, hn = tree_on_gpu(pos, mass, codes)
     soft = 0.5 / 32
     t = np.random.default_rng(2).choice(n, 1024, replace=False)
     d = direct_gpu(pos, mass, t, soft)
     prev = None
     for theta in (0.7, 0.5, 0.3):
-        g, stats, st = grouped(pos, (ch, nodes), theta, soft, 1)
+        g, stats, st = grouped(pos, codes, mass, theta, soft, 1)
         assert st == 0
         e = rel_err(g[t].astype(np.float64), d)
         p99 = np.percentile(e, 99)
@@ -501,14 +532,12 @@ def test_grouped_periodic_mac_accuracy():
     assert prev < 0.1
 
 
-def test_grouped_per_group_theta():
+def test_grouped_per_bucket_theta():
     pos, _, codes = sorted_case(16, 2, 1)
     n = codes.size
     mass = np.full(n, 1.0 / n, np.float32)
-    ch, root, nodes, hn = tree_on_gpu(pos, mass, codes)
-    groups = (n + 31) // 32
-    a, _, _ = grouped(pos, (ch, nodes), 0.6, 0.03, 1)
-    b, _, _ = grouped(pos, (ch, nodes), 0.1, 0.03, 1, tpg=np.full(groups, 0.6))
+    a, _, _ = grouped(pos, codes, mass, 0.6, 0.03, 1)
+    b, _, _ = grouped(pos, codes, mass, 0.1, 0.03, 1, tpg=np.full(n, 0.6))
     np.testing.assert_array_equal(a, b)
 
 
