@@ -49,7 +49,7 @@ class OctreeManager:
             # traversal records and boxes, node ranges and the bucket table
             self.node_table = torch.empty((4, m, 4), dtype=torch.float32, device=dev)
             self.ranges = torch.zeros((max(self.n - 1, 1), 2), dtype=torch.int32, device=dev)
-            self.workspace = torch.zeros(4 + 2 * max(self.n, 1), dtype=torch.int32, device=dev)
+            self.workspace = torch.zeros(4 + 4 * max(self.n, 1), dtype=torch.int32, device=dev)
             self.bucket = int(bucket)
 
     def _stream(self):

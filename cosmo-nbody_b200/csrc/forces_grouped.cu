@@ -43,7 +43,7 @@ struct GroupedParams {
     const float4 *aabb;  // [2*M]: (min, 0), (max, 0)
     float *force;        // [N,3]
     int32_t *ws;         // [0] bucket count, [1] work counter, [2] max stack depth
-    const int2 *buckets; // (first body, count)
+    const int4 *buckets; // (first body, count, subtree node, 0)
     const float *theta_per_bucket;  // may be null
     float theta;
     float G, soft2, box;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
         if (lane == 0) g = atomicAdd(P.ws + 1, 1);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= n_buckets) break;
-        const int2 bk = P.buckets[g];
+        const int4 bk = P.buckets[g];
         const int count = bk.y;
         float x[BPL], y[BPL], z[BPL];
         bool valid[BPL];
@@ -353,7 +353,7 @@ static int grouped_common(GroupedParams &P, const float *px, const float *py, co
     P.aabb = P.rec + 2 * m;
     P.force = force;
     P.ws = workspace;
-    P.buckets = reinterpret_cast<const int2 *>(workspace + 4);
+    P.buckets = reinterpret_cast<const int4 *>(workspace + 4);
     P.theta_per_bucket = theta_per_bucket;
     P.G = (float)G;
     P.box = 1.0f;

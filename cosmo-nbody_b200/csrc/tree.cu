@@ -81,7 +81,7 @@ __global__ void __launch_bounds__(256) k_make_buckets(const int2 *__restrict__ r
                                                       const int32_t *__restrict__ parents,
                                                       int64_t n, int max_size,
                                                       int32_t *__restrict__ ws,
-                                                      int2 *__restrict__ buckets,
+                                                      int4 *__restrict__ buckets,
                                                       const uint64_t *__restrict__ codes,
                                                       int box_shift) {
     const int64_t m = 2 * n - 1;
@@ -108,7 +108,7 @@ __global__ void __launch_bounds__(256) k_make_buckets(const int2 *__restrict__ r
         }
         if (top) {
             const int slot = atomicAdd(ws, 1);
-            buckets[slot] = make_int2(lo, size);
+            buckets[slot] = make_int4(lo, size, (int)v, 0);
         }
     }
 }
@@ -398,11 +398,11 @@ static int make_buckets(const int32_t *ranges, const int32_t *parents, const uin
     if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return CNB_E_INVALID_ARG;
     cudaStream_t st = as_stream(stream);
     CNB_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
-    int2 *buckets = reinterpret_cast<int2 *>(workspace + 4);
+    int4 *buckets = reinterpret_cast<int4 *>(workspace + 4);
     if (n == 0) return CNB_OK;
     if (n == 1) {
         const int32_t one[4] = {1, 0, 0, 0};
-        const int32_t b[2] = {0, 1};
+        const int32_t b[4] = {0, 1, 0, 0};
         CNB_CUDA(cudaMemcpyAsync(workspace, one, sizeof(one), cudaMemcpyHostToDevice, st));
         CNB_CUDA(cudaMemcpyAsync(buckets, b, sizeof(b), cudaMemcpyHostToDevice, st));
         return CNB_OK;

@@ -174,9 +174,9 @@ int cnb_build_tree_ranges(const uint64_t *codes, int32_t *children, int32_t *par
 
 /* Bucket table for cnb_forces_grouped (no reference counterpart): the
  * maximal subtrees holding at most max_size bodies.  workspace (device,
- * 16-byte aligned) is int32 [4 + 2N]: [0] bucket count, [1] work counter,
+ * 16-byte aligned) is int32 [4 + 4N]: [0] bucket count, [1] work counter,
  * [2] deepest node stack seen by the traversal, [3] unused, then one
- * (first body, count) pair per bucket. */
+ * (first body, count, subtree node, 0) record per bucket. */
 int cnb_make_buckets(const int32_t *ranges, const int32_t *parents, int64_t n, int max_size,
                      int32_t *workspace, void *stream);
 

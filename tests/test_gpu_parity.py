@@ -443,7 +443,7 @@ def grouped(pos, codes, mass, theta, soft, mac, tpg=None, bpl=1, want_ws=False, 
     table = torch.empty((4, m, 4), dtype=torch.float32, device="cuda")
     lib().call("cnb_pack_nodes", *(t.data_ptr() for t in nodes), ch.data_ptr(), table.data_ptr(), m,
                stream())
-    ws = torch.zeros(4 + 2 * n, dtype=torch.int32, device="cuda")
+    ws = torch.zeros(4 + 4 * n, dtype=torch.int32, device="cuda")
     lib().call("cnb_make_buckets", rng_.data_ptr(), par.data_ptr(), n, 32 * bpl, ws.data_ptr(), stream())
     F = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
     stats = torch.zeros(2, dtype=torch.int64, device="cuda")
@@ -487,7 +487,7 @@ def test_buckets_partition_the_bodies(bpl):
     _, _, st, ws = grouped(pos, codes, mass, 0.5, 0.01, 0, bpl=bpl, want_ws=True)
     assert st == 0
     nb = ws[0]
-    b = ws[4:4 + 2 * nb].reshape(nb, 2)
+    b = ws[4:4 + 4 * nb].reshape(nb, 4)
     assert b[:, 1].max() <= 32 * bpl and b[:, 1].min() >= 1
     order = np.argsort(b[:, 0])
     starts, counts = b[order, 0], b[order, 1]
