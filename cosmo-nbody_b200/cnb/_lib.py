@@ -32,6 +32,7 @@ PREC_F32 = 0
 PREC_F64 = 1
 UPWARD_PLAIN = 0
 UPWARD_COMPENSATED = 1
+MLP_PARAMS = 5057
 
 _p = C.c_void_p
 _i64 = C.c_int64
@@ -74,6 +75,12 @@ SIGNATURES = {
     "cnb_forces_grouped_boxes": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p, _int, _p, _p, _p, _int, _int,
                                         _d, _p, _p, _p]),
     "cnb_integrate_boxes": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _int, _i64, _p, _p]),
+    "cnb_bucket_features": (_int, [_p, _p, _p, _i64, _p, _int, _p]),
+    "cnb_controller_theta": (_int, [_p, _p, _p, _i64, _p, _p, _int, _p]),
+    "cnb_mlp_predict": (_int, [_p, _int, _p, _p, _p]),
+    "cnb_mlp_grad": (_int, [_p, _p, _int, _p, _f, _p, _p, _p, _p]),
+    "cnb_adam_step": (_int, [_p, _p, _p, _p, _int, _f, _f, _f, _f, _int, _p]),
+    "cnb_to_bf16": (_int, [_p, _p, _int, _p]),
     "cnb_direct_sum_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_fma_probe": (_int, [_p, _i64, _int, _p]),
 }

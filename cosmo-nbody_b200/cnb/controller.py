@@ -1,0 +1,225 @@
+"""Learned opening-angle controller (no reference counterpart).
+
+A small network (12 -> 64 -> 64 -> 1, SiLU, bfloat16 weights at inference,
+float32 accumulation) predicts each bucket's opening angle in [0.2, 1.0]
+from features of the bucket's subtree and three of its ancestors.  All of it
+runs in libcnb (csrc/controller.cu): the fused feature + inference kernel,
+and the training kernels (forward/backward, parameter gradients, Adam).
+
+Training pairs come from the batched boxes (cnb.core.batched): for sampled
+buckets the plain fixed-theta traversal is run at every theta of a grid and
+compared with the float64 direct sum; a bucket's label is the largest theta
+whose error stays within the budget.  Plain fixed-theta Barnes-Hut remains
+the fallback (no weights: theta_per_bucket = None) and the reference for the
+error budget.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import _lib
+from .core.batched import BatchedBoxes
+
+N_IN, N_H = 12, 64
+N_PARAMS = _lib.MLP_PARAMS
+THETA_GRID = (0.2, 0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 0.9, 1.0)
+
+
+def _st():
+    return int(torch.cuda.current_stream().cuda_stream)
+
+
+class ThetaController:
+    def __init__(self, device="cuda", seed=0):
+        self.device = torch.device(device)
+        rng = np.random.default_rng(seed)
+        p = np.zeros(N_PARAMS, np.float32)
+        o = 0
+        for fan_in, fan_out in ((N_IN, N_H), (N_H, N_H), (N_H, 1)):
+            lim = np.sqrt(6.0 / (fan_in + fan_out))
+            p[o:o + fan_in * fan_out] = rng.uniform(-lim, lim, fan_in * fan_out)
+            o += fan_in * fan_out + fan_out   # weights then zero biases
+        self.params = torch.from_numpy(p).to(self.device)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.t = 0
+        self.mean = torch.zeros(N_IN, device=self.device)
+        self.std = torch.ones(N_IN, device=self.device)
+        self.weights_bf16 = None
+
+    # -------------------------------------------------------------- training
+    def set_normalisation(self, X):
+        """Fold a feature standardisation into the first layer later (export)."""
+        self.mean = X.mean(0)
+        self.std = X.std(0).clamp_min(1e-6)
+
+    def _norm(self, X):
+        return ((X - self.mean) / self.std).contiguous()
+
+    def grad(self, X, y, over_weight=4.0):
+        """Loss and gradient on the GPU (libcnb kernels) for normalised features X."""
+        n = X.shape[0]
+        scratch = torch.empty(4 * N_H * n + n, dtype=torch.float32, device=self.device)
+        g = torch.empty(N_PARAMS, dtype=torch.float32, device=self.device)
+        loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        _lib.call("cnb_mlp_grad", X.data_ptr(), y.data_ptr(), n, self.params.data_ptr(),
+                  float(over_weight), scratch.data_ptr(), g.data_ptr(), loss.data_ptr(), _st())
+        return loss, g
+
+    def train(self, X, y, steps=1500, lr=3e-3, over_weight=4.0, log_every=0):
+        """Full-batch Adam on (features X [n,12], labels y [n]); returns the loss curve."""
+        X = X.to(self.device, torch.float32)
+        y = y.to(self.device, torch.float32).contiguous()
+        self.set_normalisation(X)
+        Xn = self._norm(X)
+        n = Xn.shape[0]
+        scratch = torch.empty(4 * N_H * n + n, dtype=torch.float32, device=self.device)
+        g = torch.empty(N_PARAMS, dtype=torch.float32, device=self.device)
+        loss = torch.zeros(1, dtype=torch.float32, device=self.device)
+        curve = []
+        for it in range(steps):
+            _lib.call("cnb_mlp_grad", Xn.data_ptr(), y.data_ptr(), n, self.params.data_ptr(),
+                      float(over_weight), scratch.data_ptr(), g.data_ptr(), loss.data_ptr(), _st())
+            self.t += 1
+            _lib.call("cnb_adam_step", self.params.data_ptr(), g.data_ptr(), self.m.data_ptr(),
+                      self.v.data_ptr(), N_PARAMS, float(lr), 0.9, 0.999, 1e-8, self.t, _st())
+            if it % 50 == 0 or it == steps - 1:
+                curve.append(float(loss.item()))
+        self.export()
+        return curve
+
+    def predict(self, X):
+        """theta for raw features X (float32 weights)."""
+        Xn = self._norm(X.to(self.device, torch.float32))
+        out = torch.empty(Xn.shape[0], dtype=torch.float32, device=self.device)
+        _lib.call("cnb_mlp_predict", Xn.data_ptr(), Xn.shape[0], self.params.data_ptr(),
+                  out.data_ptr(), _st())
+        return out
+
+    # -------------------------------------------------------------- inference
+    def folded_params(self):
+        """Parameters with the feature standardisation folded into layer 1."""
+        p = self.params.clone()
+        W1 = p[:N_H * N_IN].view(N_H, N_IN)
+        b1 = p[N_H * N_IN:N_H * N_IN + N_H]
+        b1 -= (W1 * (self.mean / self.std)).sum(1)
+        W1 /= self.std
+        return p
+
+    def export(self):
+        """bfloat16 weights for the fused inference kernel."""
+        p = self.folded_params()
+        self.weights_bf16 = torch.empty(N_PARAMS, dtype=torch.bfloat16, device=self.device)
+        _lib.call("cnb_to_bf16", p.data_ptr(), self.weights_bf16.data_ptr(), N_PARAMS, _st())
+        return self.weights_bf16
+
+    def theta_for_buckets(self, node_table, parents, workspace, n, out=None, scale=1.0):
+        """theta per bucket slot of a built tree (fused features + network)."""
+        if self.weights_bf16 is None:
+            self.export()
+        max_b = (workspace.numel() - 4) // 4
+        if out is None:
+            out = torch.empty(max_b, dtype=torch.float32, device=self.device)
+        _lib.call("cnb_controller_theta", node_table.data_ptr(), parents.data_ptr(),
+                  workspace.data_ptr(), n, self.weights_bf16.data_ptr(), out.data_ptr(), max_b, _st())
+        if scale != 1.0:
+            out.mul_(scale).clamp_(0.2, 1.0)
+        return out
+
+    def save(self, path):
+        np.savez(path, params=self.params.cpu().numpy(), mean=self.mean.cpu().numpy(),
+                 std=self.std.cpu().numpy())
+
+    def load(self, path):
+        d = np.load(path)
+        self.params = torch.from_numpy(d["params"]).to(self.device)
+        self.mean = torch.from_numpy(d["mean"]).to(self.device)
+        self.std = torch.from_numpy(d["std"]).to(self.device)
+        self.export()
+        return self
+
+
+def bucket_features(node_table, parents, workspace, n):
+    max_b = (workspace.numel() - 4) // 4
+    out = torch.empty((max_b, N_IN), dtype=torch.float32, device=node_table.device)
+    _lib.call("cnb_bucket_features", node_table.data_ptr(), parents.data_ptr(), workspace.data_ptr(),
+              n, out.data_ptr(), max_b, _st())
+    nb = int(workspace[0].item())
+    return out[:nb]
+
+
+def direct_sum(pos, mass, targets, G, soft):
+    """float64 minimum-image direct sum (libcnb) for `targets` of one box."""
+    T = targets.to(torch.int64).contiguous()
+    out = torch.empty((T.numel(), 3), dtype=torch.float64, device=pos[0].device)
+    _lib.call("cnb_direct_sum_f64", *(p.data_ptr() for p in pos), mass.data_ptr(), pos[0].numel(),
+              T.data_ptr(), T.numel(), float(G), float(soft), out.data_ptr(), _st())
+    return out
+
+
+def make_labels(bb: BatchedBoxes, theta_grid=THETA_GRID, budget=None, per_box=48, seed=0,
+                error="rms"):
+    """(features, labels, info) for sampled buckets of every box of `bb`.
+
+    For every theta of the grid the plain traversal runs with that theta in
+    every bucket; each sampled bucket's error is the largest force error of
+    its bodies against the float64 direct sum of its box, either relative to
+    the body's own acceleration (error="relative") or to the box's RMS
+    acceleration (error="rms").  The label is the largest theta whose error
+    is within `budget`; budget None means the 99th-percentile error of plain
+    theta = 0.5 over all sampled bodies.  Buckets that miss the budget even at
+    the smallest theta get the smallest theta (counted in info["saturated"])."""
+    rng = np.random.default_rng(seed)
+    bb.sort_and_build()
+    feats = bucket_features(bb.table, bb.parent, bb.workspace, bb.n)
+    bk = bb.buckets().cpu().numpy()
+    box_of = np.searchsorted(bb.offsets, bk[:, 0], side="right") - 1
+    chosen = []
+    for b in range(bb.n_boxes):
+        idx = np.nonzero(box_of == b)[0]
+        chosen.extend(rng.choice(idx, min(per_box, idx.size), replace=False).tolist())
+    chosen = np.array(sorted(chosen))
+    # bodies of the chosen buckets and their float64 direct sums, box by box
+    bodies, owner = [], []
+    ref = []
+    for b in range(bb.n_boxes):
+        sel = chosen[box_of[chosen] == b]
+        if sel.size == 0:
+            continue
+        t = np.concatenate([np.arange(bk[g, 0], bk[g, 0] + bk[g, 1]) for g in sel])
+        o = np.concatenate([np.full(bk[g, 1], k) for k, g in zip(np.searchsorted(chosen, sel), sel)])
+        sl = bb.box_slice(b)
+        local = torch.from_numpy(t - sl.start).to(bb.device)
+        soft = 0.5 / bb.boxes[b]["n_grid"]
+        ref.append(direct_sum([p[sl] for p in bb.pos], bb.mass[sl], local, bb.G, soft))
+        bodies.append(t)
+        owner.append(o)
+    box_rms = [r.norm(dim=1).pow(2).mean().sqrt().expand(r.shape[0]) for r in ref]
+    bodies = torch.from_numpy(np.concatenate(bodies)).to(bb.device)
+    owner = np.concatenate(owner)
+    ref = torch.cat(ref)
+    refn = ref.norm(dim=1) if error == "relative" else torch.cat(box_rms)
+    errs = np.zeros((len(theta_grid), chosen.size))
+    body_err = {}
+    nb = bk.shape[0]
+    cost = []
+    for k, th in enumerate(theta_grid):
+        tpb = torch.full((max(nb, 1),), float(th), dtype=torch.float32, device=bb.device)
+        bb.stats.zero_()
+        bb.compute_forces(theta_per_bucket=tpb)
+        e = ((bb.force[bodies].double() - ref).norm(dim=1) / refn).cpu().numpy()
+        body_err[th] = e
+        np.maximum.at(errs[k], owner, e)
+        cost.append(float(bb.stats[0].item()) / bb.n)
+    bb.check()
+    if budget is None:
+        budget = float(np.percentile(body_err[0.5], 99))
+    ok = errs <= budget
+    labels = np.full(chosen.size, theta_grid[0], np.float32)
+    for k, th in enumerate(theta_grid):
+        labels[ok[k]] = th      # ascending grid: the largest passing theta wins
+    info = dict(budget=budget, saturated=float(np.mean(~ok.any(axis=0))), cost_per_theta=cost,
+                n_samples=int(chosen.size), label_hist=np.bincount(
+                    np.searchsorted(theta_grid, labels), minlength=len(theta_grid)).tolist())
+    return feats[torch.from_numpy(chosen).to(bb.device)], torch.from_numpy(labels).to(bb.device), info

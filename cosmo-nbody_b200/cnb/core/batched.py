@@ -104,7 +104,7 @@ class BatchedBoxes:
         self.workspace = z(4 + 4 * n, dt=torch.int32)
         self.box_roots = z(self.n_boxes, dt=torch.int32)
         self.force = z(n, 3)
-        self.stats = z(2, dt=torch.int64)
+        self.stats = z(4, dt=torch.int64)
         self.theta_per_bucket = None
         self._ctx = SortContext(n)
         self._graph = None

@@ -50,7 +50,10 @@ class SimulationEngine:
         self.node_to_cache = torch.full((self.tree_manager.n_nodes,), -1, dtype=torch.int32,
                                         device=state.device)
         self.theta_per_group = None   # float32 per bucket slot (device), grouped mode only
-        self.stats = torch.zeros(2, dtype=torch.int64, device=state.device)
+        # learned opening-angle controller (cnb.controller.ThetaController); None = plain theta
+        self.controller = None
+        self.controller_scale = 1.0
+        self.stats = torch.zeros(4, dtype=torch.int64, device=state.device)
         self.mac = MACS[getattr(config, "MAC", "ref_x")]
         # periodic test: image-ambiguous nodes of at most SLAB_BODIES bodies' mass are applied
         # with the per-pair minimum image (0 = exact)
@@ -68,6 +71,11 @@ class SimulationEngine:
         status = status_buffer(s.device.index).data_ptr()
         px, py, pz = s.pos
         if self.force_mode == "grouped":
+            if self.controller is not None:
+                # learned per-bucket theta (fused features + network on the GPU)
+                self.theta_per_group = self.controller.theta_for_buckets(
+                    tm.node_table, tm.parent, tm.workspace, s.n, out=self.theta_per_group,
+                    scale=self.controller_scale)
             tpg = self.theta_per_group
             _lib.call("cnb_forces_grouped", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                       tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,

@@ -1,0 +1,354 @@
+// controller.cu -- learned opening-angle controller (no reference
+// counterpart): bucket features, the fused feature + MLP inference kernel,
+// and the training kernels (forward/backward, parameter gradients, Adam).
+//
+// Network: 12 inputs -> 64 -> 64 -> 1, SiLU hidden activations, output
+// theta = THETA_LO + (THETA_HI - THETA_LO) * sigmoid(z), i.e. clipped to
+// [0.2, 1.0].  Parameters (CNB_MLP_PARAMS floats, this order):
+//   W1[64][12], b1[64], W2[64][64], b2[64], w3[64], b3.
+// Inference keeps the weights in bfloat16 and accumulates in float32;
+// training keeps float32 master weights.
+//
+// Features of a bucket (its subtree node v, ancestors p1..p3), lengths in
+// units of the box's mean body spacing s = (body mass)^(1/3):
+//   f0  log2(extent(v) / s)                f1  log2(bodies) / 5
+//   f2  log2(density(v) / mean density)
+//   f3+3k..f5+3k (k = 0..2, ancestor p_{k+1}):
+//       log2(extent(p) / extent(v)), log2(mass(p) / mass(v)),
+//       |com(p) - com(v)| / extent(p)
+#include <cuda_bf16.h>
+
+#include "common.cuh"
+
+namespace cnb {
+
+constexpr int kIn = 12, kH = 64;
+constexpr int kOffW1 = 0, kOffB1 = kOffW1 + kH * kIn, kOffW2 = kOffB1 + kH,
+              kOffB2 = kOffW2 + kH * kH, kOffW3 = kOffB2 + kH, kOffB3 = kOffW3 + kH;
+constexpr int kParams = kOffB3 + 1;  // 5057
+constexpr float kThetaLo = 0.2f, kThetaHi = 1.0f;
+static_assert(kParams == CNB_MLP_PARAMS, "parameter count");
+
+__device__ __forceinline__ float sigmoidf_(float x) { return 1.f / (1.f + __expf(-x)); }
+__device__ __forceinline__ float siluf_(float x) { return x * sigmoidf_(x); }
+
+__device__ __forceinline__ float node_extent(const float4 *aabb, int v) {
+    const float4 lo = aabb[2 * v], hi = aabb[2 * v + 1];
+    return fmaxf(hi.x - lo.x, fmaxf(hi.y - lo.y, hi.z - lo.z));
+}
+
+__device__ void bucket_features(const float4 *__restrict__ rec, const float4 *__restrict__ aabb,
+                                const int32_t *__restrict__ parents, int4 bk, float f[kIn]) {
+    const int v = bk.z;
+    const float4 A = rec[2 * v];
+    const float m_body = A.w / (float)bk.y;
+    const float s = cbrtf(fmaxf(m_body, 1e-30f));  // mean spacing of the box (unit cube)
+    const float4 lo = aabb[2 * v], hi = aabb[2 * v + 1];
+    const float ext = fmaxf(node_extent(aabb, v), 1e-3f * s);
+    const float vol = (hi.x - lo.x + s) * (hi.y - lo.y + s) * (hi.z - lo.z + s);
+    f[0] = __log2f(ext / s);
+    f[1] = __log2f((float)bk.y) * 0.2f;
+    f[2] = __log2f((float)bk.y * s * s * s / vol);
+    int p = v;
+    for (int k = 0; k < 3; ++k) {
+        const int q = parents[p];
+        if (q >= 0) p = q;
+        const float4 P = rec[2 * p];
+        const float pe = fmaxf(node_extent(aabb, p), ext);
+        const float dx = P.x - A.x, dy = P.y - A.y, dz = P.z - A.z;
+        f[3 + 3 * k] = __log2f(pe / ext);
+        f[4 + 3 * k] = __log2f(fmaxf(P.w, A.w) / A.w);
+        f[5 + 3 * k] = sqrtf(dx * dx + dy * dy + dz * dz) / pe;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_features(const float4 *__restrict__ rec,
+                                                  const float4 *__restrict__ aabb,
+                                                  const int32_t *__restrict__ parents,
+                                                  const int32_t *__restrict__ ws,
+                                                  float *__restrict__ out, int max_buckets) {
+    const int nb = min(ws[0], max_buckets);
+    const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
+        float f[kIn];
+        bucket_features(rec, aabb, parents, buckets[g], f);
+#pragma unroll
+        for (int k = 0; k < kIn; ++k) out[(int64_t)g * kIn + k] = f[k];
+    }
+}
+
+// z = network output before the output squashing, float32 weights in
+// shared memory.  Hidden unit j of layer 1 is formed once and scattered into
+// the 64 layer-2 accumulators, so only those stay in registers.
+__device__ __forceinline__ float mlp_forward(const float *__restrict__ w, const float x[kIn]) {
+    float a2[kH];
+#pragma unroll
+    for (int k = 0; k < kH; ++k) a2[k] = w[kOffB2 + k];
+#pragma unroll 1
+    for (int j = 0; j < kH; ++j) {
+        float a = w[kOffB1 + j];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) a = fmaf(w[kOffW1 + j * kIn + i], x[i], a);
+        const float h = siluf_(a);
+#pragma unroll
+        for (int k = 0; k < kH; ++k) a2[k] = fmaf(w[kOffW2 + k * kH + j], h, a2[k]);
+    }
+    float z = w[kOffB3];
+#pragma unroll
+    for (int k = 0; k < kH; ++k) z = fmaf(w[kOffW3 + k], siluf_(a2[k]), z);
+    return z;
+}
+
+__device__ __forceinline__ float theta_of(float z) {
+    return kThetaLo + (kThetaHi - kThetaLo) * sigmoidf_(z);
+}
+
+// Fused inference: features of each bucket and the network on bfloat16
+// weights (converted once per block into float32 shared memory).
+__global__ void __launch_bounds__(256) k_controller(const float4 *__restrict__ rec,
+                                                    const float4 *__restrict__ aabb,
+                                                    const int32_t *__restrict__ parents,
+                                                    const int32_t *__restrict__ ws,
+                                                    const __nv_bfloat16 *__restrict__ wbf,
+                                                    float *__restrict__ theta, int max_buckets) {
+    __shared__ float w[kParams];
+    for (int i = threadIdx.x; i < kParams; i += blockDim.x) w[i] = __bfloat162float(wbf[i]);
+    __syncthreads();
+    const int nb = min(ws[0], max_buckets);
+    const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
+        float f[kIn];
+        bucket_features(rec, aabb, parents, buckets[g], f);
+        theta[g] = theta_of(mlp_forward(w, f));
+    }
+}
+
+// Inference on given features with float32 weights (training evaluation).
+__global__ void __launch_bounds__(256) k_mlp_predict(const float *__restrict__ x, int n,
+                                                     const float *__restrict__ wg,
+                                                     float *__restrict__ theta) {
+    __shared__ float w[kParams];
+    for (int i = threadIdx.x; i < kParams; i += blockDim.x) w[i] = wg[i];
+    __syncthreads();
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        float f[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) f[i] = x[(int64_t)s * kIn + i];
+        theta[s] = theta_of(mlp_forward(w, f));
+    }
+}
+
+// Training, phase 1 (one thread per sample): forward pass and the backward
+// pass down to the pre-activation gradients.  Loss per sample:
+//   L = c * (theta - y)^2,  c = over_weight if theta > y else 1,
+// averaged over the n samples (over-estimating theta costs accuracy, so it
+// can be weighted up).  Writes H1, DA1, H2, DA2 ([n, 64] each), DZ [n] and
+// adds the loss sum into *loss.
+__global__ void __launch_bounds__(128) k_mlp_backward_acts(
+    const float *__restrict__ x, const float *__restrict__ y, int n, const float *__restrict__ wg,
+    float over_weight, float *__restrict__ H1, float *__restrict__ DA1, float *__restrict__ H2,
+    float *__restrict__ DA2, float *__restrict__ DZ, float *__restrict__ loss) {
+    __shared__ float w[kParams];
+    for (int i = threadIdx.x; i < kParams; i += blockDim.x) w[i] = wg[i];
+    __syncthreads();
+    float lsum = 0.f;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+        float f[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) f[i] = x[(int64_t)s * kIn + i];
+        float* h1row = H1 + (int64_t)s * kH;
+        float* da1row = DA1 + (int64_t)s * kH;
+        float a2[kH];
+#pragma unroll
+        for (int k = 0; k < kH; ++k) a2[k] = w[kOffB2 + k];
+#pragma unroll 1
+        for (int j = 0; j < kH; ++j) {
+            float a = w[kOffB1 + j];
+#pragma unroll
+            for (int i = 0; i < kIn; ++i) a = fmaf(w[kOffW1 + j * kIn + i], f[i], a);
+            const float h = siluf_(a);
+            h1row[j] = h;
+            da1row[j] = a;  // layer-1 pre-activation, turned into its gradient below
+#pragma unroll
+            for (int k = 0; k < kH; ++k) a2[k] = fmaf(w[kOffW2 + k * kH + j], h, a2[k]);
+        }
+        float z = w[kOffB3];
+#pragma unroll
+        for (int k = 0; k < kH; ++k) {
+            const float h = siluf_(a2[k]);
+            H2[(int64_t)s * kH + k] = h;
+            z = fmaf(w[kOffW3 + k], h, z);
+        }
+        const float sg = sigmoidf_(z);
+        const float th = kThetaLo + (kThetaHi - kThetaLo) * sg;
+        const float diff = th - y[s];
+        const float c = diff > 0.f ? over_weight : 1.f;
+        lsum += c * diff * diff;
+        const float dz = (2.f * c * diff / (float)n) * (kThetaHi - kThetaLo) * sg * (1.f - sg);
+        DZ[s] = dz;
+#pragma unroll
+        for (int k = 0; k < kH; ++k) {
+            const float sa = sigmoidf_(a2[k]);
+            a2[k] = dz * w[kOffW3 + k] * sa * (1.f + a2[k] * (1.f - sa));  // now dL/da2
+            DA2[(int64_t)s * kH + k] = a2[k];
+        }
+#pragma unroll 1
+        for (int j = 0; j < kH; ++j) {
+            float dh = 0.f;
+#pragma unroll
+            for (int k = 0; k < kH; ++k) dh = fmaf(w[kOffW2 + k * kH + j], a2[k], dh);
+            const float a = da1row[j];
+            const float sa = sigmoidf_(a);
+            da1row[j] = dh * sa * (1.f + a * (1.f - sa));
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, lsum / (float)n);
+}
+
+// Training, phase 2: parameter gradients as sums over samples.  Block r < 64
+// computes row r of W1 (12 inputs) and b1; block 64 + r row r of W2 and b2;
+// block 128 computes w3 and b3.  Threads stride over samples; each output
+// is reduced in shared memory.  grad must hold CNB_MLP_PARAMS floats.
+__global__ void __launch_bounds__(256) k_mlp_param_grads(
+    const float *__restrict__ x, int n, const float *__restrict__ H1, const float *__restrict__ DA1,
+    const float *__restrict__ H2, const float *__restrict__ DA2, const float *__restrict__ DZ,
+    float *__restrict__ grad) {
+    __shared__ float red[kH + 1][8];
+    const int r = blockIdx.x;
+    float acc[kH + 1];
+#pragma unroll
+    for (int k = 0; k <= kH; ++k) acc[k] = 0.f;
+    int cols = 0;
+    const float *rowsrc = nullptr;  // per-sample scalar multiplier (column r)
+    const float *insrc = nullptr;   // per-sample input vector
+    int in_stride = 0;
+    if (r < kH) {
+        cols = kIn; rowsrc = DA1; insrc = x; in_stride = kIn;
+    } else if (r < 2 * kH) {
+        cols = kH; rowsrc = DA2; insrc = H1; in_stride = kH;
+    } else {
+        cols = kH; rowsrc = DZ; insrc = H2; in_stride = kH;
+    }
+    const int rr = r < 2 * kH ? (r % kH) : 0;
+    for (int s = threadIdx.x; s < n; s += blockDim.x) {
+        const float d = (r < 2 * kH) ? rowsrc[(int64_t)s * kH + rr] : rowsrc[s];
+#pragma unroll
+        for (int k = 0; k < kH; ++k)
+            if (k < cols) acc[k] = fmaf(d, insrc[(int64_t)s * in_stride + k], acc[k]);
+        acc[kH] += d;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k <= kH; ++k) {
+        float v = acc[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x <= kH) {
+        const int k = threadIdx.x;
+        if (k < cols || k == kH) {
+            float v = 0.f;
+            for (int w8 = 0; w8 < (int)(blockDim.x >> 5); ++w8) v += red[k][w8];
+            if (r < kH) {
+                if (k < kH) grad[kOffW1 + rr * kIn + k] = v; else grad[kOffB1 + rr] = v;
+            } else if (r < 2 * kH) {
+                if (k < kH) grad[kOffW2 + rr * kH + k] = v; else grad[kOffB2 + rr] = v;
+            } else {
+                if (k < kH) grad[kOffW3 + k] = v; else grad[kOffB3] = v;
+            }
+        }
+    }
+}
+
+__global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
+                       float *__restrict__ v, int n, float lr, float b1, float b2, float eps,
+                       float c1, float c2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.f - b1) * gi;
+        const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    }
+}
+
+__global__ void k_to_bf16(const float *__restrict__ src, __nv_bfloat16 *__restrict__ dst, int n) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = __float2bfloat16_rn(src[i]);
+}
+
+}  // namespace cnb
+
+using namespace cnb;
+
+extern "C" int cnb_bucket_features(const float *node_table, const int32_t *parents,
+                                   const int32_t *workspace, int64_t n, float *features,
+                                   int max_buckets, void *stream) {
+    if (n < 1 || !node_table || !parents || !workspace || !features || max_buckets < 0)
+        return CNB_E_INVALID_ARG;
+    const int64_t m = 2 * n - 1;
+    const float4 *rec = reinterpret_cast<const float4 *>(node_table);
+    k_features<<<grid_for(max_buckets, 256), 256, 0, as_stream(stream)>>>(
+        rec, rec + 2 * m, parents, workspace, features, max_buckets);
+    return launch_status();
+}
+
+extern "C" int cnb_controller_theta(const float *node_table, const int32_t *parents,
+                                    const int32_t *workspace, int64_t n,
+                                    const void *weights_bf16, float *theta, int max_buckets,
+                                    void *stream) {
+    if (n < 1 || !node_table || !parents || !workspace || !weights_bf16 || !theta ||
+        max_buckets < 0)
+        return CNB_E_INVALID_ARG;
+    const int64_t m = 2 * n - 1;
+    const float4 *rec = reinterpret_cast<const float4 *>(node_table);
+    k_controller<<<grid_for(max_buckets, 256, 148 * 4), 256, 0, as_stream(stream)>>>(
+        rec, rec + 2 * m, parents, workspace,
+        reinterpret_cast<const __nv_bfloat16 *>(weights_bf16), theta, max_buckets);
+    return launch_status();
+}
+
+extern "C" int cnb_mlp_predict(const float *features, int n, const float *weights, float *theta,
+                               void *stream) {
+    if (n < 0 || (n > 0 && (!features || !weights || !theta))) return CNB_E_INVALID_ARG;
+    if (n == 0) return CNB_OK;
+    k_mlp_predict<<<grid_for(n, 256, 148 * 4), 256, 0, as_stream(stream)>>>(features, n, weights,
+                                                                            theta);
+    return launch_status();
+}
+
+extern "C" int cnb_mlp_grad(const float *features, const float *labels, int n,
+                            const float *weights, float over_weight, float *scratch,
+                            float *grad, float *loss, void *stream) {
+    if (n < 1 || !features || !labels || !weights || !scratch || !grad || !loss)
+        return CNB_E_INVALID_ARG;
+    cudaStream_t st = as_stream(stream);
+    float *H1 = scratch, *DA1 = H1 + (int64_t)n * kH, *H2 = DA1 + (int64_t)n * kH,
+          *DA2 = H2 + (int64_t)n * kH, *DZ = DA2 + (int64_t)n * kH;
+    CNB_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
+    k_mlp_backward_acts<<<grid_for(n, 128, 148 * 8), 128, 0, st>>>(
+        features, labels, n, weights, over_weight, H1, DA1, H2, DA2, DZ, loss);
+    CNB_TRY(launch_status());
+    k_mlp_param_grads<<<2 * kH + 1, 256, 0, st>>>(features, n, H1, DA1, H2, DA2, DZ, grad);
+    return launch_status();
+}
+
+extern "C" int cnb_adam_step(float *params, const float *grad, float *m, float *v, int n,
+                             float lr, float beta1, float beta2, float eps, int t, void *stream) {
+    if (n < 1 || !params || !grad || !m || !v || t < 1) return CNB_E_INVALID_ARG;
+    const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+    k_adam<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(params, grad, m, v, n, lr, beta1,
+                                                           beta2, eps, c1, c2);
+    return launch_status();
+}
+
+extern "C" int cnb_to_bf16(const float *src, void *dst, int n, void *stream) {
+    if (n < 0 || (n > 0 && (!src || !dst))) return CNB_E_INVALID_ARG;
+    if (n == 0) return CNB_OK;
+    k_to_bf16<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
+        src, reinterpret_cast<__nv_bfloat16 *>(dst), n);
+    return launch_status();
+}

@@ -57,7 +57,8 @@ struct GroupedParams {
     int box_shift;
     const int32_t *box_roots;   // subtree root per box
     const float4 *box_params;   // (theta, softening, slab mass, 0) per box
-    unsigned long long *stats;  // [0] body-entry interactions, [1] node tests (may be null)
+    unsigned long long *stats;  // [0] body-node interactions, [1] node tests,
+                                // [2] interactions needing the per-pair image (may be null)
     int32_t *status;
 };
 
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
 #pragma unroll
         for (int b = 0; b < BPL; ++b) ax[b] = ay[b] = az[b] = 0.f;
         int top = 1, cnt = 0;
-        unsigned long long n_entries = 0;
+        unsigned long long n_entries = 0, n_wrap = 0;
         if (lane == 0) stack[0] = root;
         __syncwarp();
         // a valid tree pushes every node at most once per bucket: more rounds
@@ -226,6 +227,7 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
             }
             n_tests += (node >= 0);
             const uint32_t am = __ballot_sync(0xffffffffu, accept);
+            n_wrap += __popc(__ballot_sync(0xffffffffu, accept && E.w < 0.f));
             const uint32_t om = __ballot_sync(0xffffffffu, open);
             if (accept) list[cnt + __popc(am & lt)] = E;
             cnt += __popc(am);
@@ -266,7 +268,10 @@ __global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P
                     set_flag(P.status, CNB_FLAG_NONFINITE);
             }
         }
-        if (P.stats && lane == 0) atomicAdd(P.stats, n_entries * (unsigned long long)count);
+        if (P.stats && lane == 0) {
+            atomicAdd(P.stats, n_entries * (unsigned long long)count);
+            atomicAdd(P.stats + 2, n_wrap * (unsigned long long)count);
+        }
     }
     if (overflow && lane == 0) set_flag(P.status, CNB_FLAG_LIST_OVERFLOW);
     if (P.stats) {

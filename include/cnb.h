@@ -204,8 +204,9 @@ int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
  * (CNB_MAC_PERIODIC only): nodes whose image differs between a bucket's
  * bodies are opened unless their mass is at most slab_mass, in which case
  * they are applied with the per-pair minimum image of their CoM (0 = exact
- * minimum-image semantics).  stats (device, 2 x uint64, may be NULL)
- * accumulates [body-node interactions, node tests]. */
+ * minimum-image semantics).  stats (device, 3 x uint64, may be NULL)
+ * accumulates [body-node interactions, node tests, interactions applied
+ * with the per-pair minimum image]. */
 int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                        const float *node_table, int32_t *workspace, float *force, int64_t n,
                        double theta, const float *theta_per_bucket, int mac, int bodies_per_lane,
@@ -240,6 +241,42 @@ int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,
 int cnb_integrate_boxes(float *px, float *py, float *pz, float *vx, float *vy, float *vz,
                         const float *force, const uint64_t *codes, int box_bits, int64_t n,
                         const double *box_aHdt, void *stream);
+
+/* ---- learned opening-angle controller (no reference counterpart) ----
+ * An MLP 12 -> 64 -> 64 -> 1 (SiLU) maps features of a bucket to its theta
+ * in [0.2, 1.0].  Parameters: CNB_MLP_PARAMS float32 values, in the order
+ * W1[64][12], b1[64], W2[64][64], b2[64], w3[64], b3. */
+#define CNB_MLP_PARAMS 5057
+
+/* 12 features per bucket (float32 [buckets, 12]) from the node table,
+ * parents and the bucket table of cnb_make_buckets; at most max_buckets. */
+int cnb_bucket_features(const float *node_table, const int32_t *parents,
+                        const int32_t *workspace, int64_t n, float *features, int max_buckets,
+                        void *stream);
+
+/* Fused inference: features and the network (bfloat16 weights, float32
+ * accumulation) -> theta per bucket slot, the theta_per_bucket input of
+ * cnb_forces_grouped. */
+int cnb_controller_theta(const float *node_table, const int32_t *parents,
+                         const int32_t *workspace, int64_t n, const void *weights_bf16,
+                         float *theta, int max_buckets, void *stream);
+
+/* The network on given features with float32 weights. */
+int cnb_mlp_predict(const float *features, int n, const float *weights, float *theta,
+                    void *stream);
+
+/* Training: loss = mean over samples of c (theta - label)^2, c = over_weight
+ * where theta > label, else 1; writes the gradient (CNB_MLP_PARAMS floats)
+ * and the loss.  scratch: float32 [4 * 64 * n + n]. */
+int cnb_mlp_grad(const float *features, const float *labels, int n, const float *weights,
+                 float over_weight, float *scratch, float *grad, float *loss, void *stream);
+
+/* One Adam update of n parameters (step t >= 1). */
+int cnb_adam_step(float *params, const float *grad, float *m, float *v, int n, float lr,
+                  float beta1, float beta2, float eps, int t, void *stream);
+
+/* float32 -> bfloat16 (round to nearest even). */
+int cnb_to_bf16(const float *src, void *dst, int n, void *stream);
 
 /* Float64 minimum-image direct sum (the force law of
  * src/kernels/physics_kernels.py:118-141 over every pair) for the bodies

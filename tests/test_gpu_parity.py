@@ -446,7 +446,7 @@ def grouped(pos, codes, mass, theta, soft, mac, tpg=None, bpl=1, want_ws=False, 
     ws = torch.zeros(4 + 4 * n, dtype=torch.int32, device="cuda")
     lib().call("cnb_make_buckets", rng_.data_ptr(), par.data_ptr(), n, 32 * bpl, ws.data_ptr(), stream())
     F = torch.zeros((n, 3), dtype=torch.float32, device="cuda")
-    stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+    stats = torch.zeros(4, dtype=torch.int64, device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     T = dev(tpg.astype(np.float32)) if tpg is not None else None
     lib().call("cnb_forces_grouped", *(p.data_ptr() for p in P), table.data_ptr(), ws.data_ptr(),
