@@ -55,6 +55,9 @@ def parse():
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--accuracy-sample", type=int, default=4096)
     ap.add_argument("--cpu-sample", type=int, default=8192)
+    ap.add_argument("--no-graph", dest="graph", action="store_false",
+                    help="launch every kernel from Python instead of replaying a CUDA graph")
+    ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
     ap.add_argument("--profile", action="store_true",
                     help="timed loop only (no e2e, accuracy, CPU baseline or clock sampling)")
     return ap.parse_args()
@@ -288,42 +291,75 @@ def run_ours(args):
     for i in range(args.warmup):
         one_step(i)
     eng.check()
-    barrier(ws)
-
+    tune_report = None
+    if args.force_mode == "grouped" and not args.no_tune:
+        from cnb import autotune
+        tune_report = autotune.tune(eng)          # launch shape for this GPU / workload
+    # per-stage breakdown and interaction counts from two eager steps (untimed)
     eng.enable_stage_timing(True)
     eng.stats.zero_()
-    launches0 = _lib.launch_count()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    for i in range(2):
+        one_step(args.warmup + i)
+    stages = {k: v / 2 for k, v in eng.stage_times().items()}
+    eng.enable_stage_timing(False)
+    stats = eng.stats.cpu().numpy()
+    interactions_per_step = float(stats[0]) / 2       # body-node interactions
+    forces_ms = stages.get("forces", 0.0)
+    eng.check()
+    step0 = args.warmup + 2
+    launches_per_step = None
+    if args.graph:
+        l0 = _lib.launch_count()
+        eng.capture(splat=True)                        # 2 eager steps + a 2-step graph
+        launches_per_step = (_lib.launch_count() - l0) // 4   # captured launches are counted once
     sampler = ClockSampler(local) if not args.profile else None
     if sampler:
         sampler.__enter__()
+        t_end = time.time() + 1.0                      # pre-roll so the clock samples see load
+        while time.time() < t_end:
+            eng.replay() if args.graph else one_step(step0)
+            torch.cuda.synchronize()
     barrier(ws)
-    for k in range(args.steps):
+    launches0 = _lib.launch_count()
+    # graph mode: one replay = two steps; an odd K ends with one eager device step
+    n_iter = (args.steps + 1) // 2 if args.graph else args.steps
+    steps_done = args.steps
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(n_iter)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(n_iter)]
+    for k in range(n_iter):
         flush.zero_()
         starts[k].record()
-        one_step(args.warmup + k)
+        if not args.graph:
+            one_step(step0 + k)
+        elif 2 * k + 1 < args.steps:
+            eng.replay()
+        else:
+            eng.mvp_slots[0].copy_(eng.camera.mvp_host(eng._graph_step))
+            eng._step_device(eng.mvp_slots[0])
+            eng.a += eng.da
         ends[k].record()
     barrier(ws)
     if sampler:
         sampler.__exit__()
-    launches = (_lib.launch_count() - launches0) // args.steps
+    if not args.graph:
+        launches_per_step = (_lib.launch_count() - launches0) // args.steps
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    stages = eng.stage_times()
-    eng.enable_stage_timing(False)
     total_ms = max_over_ranks(sum(step_ms), ws)
-    stats = eng.stats.cpu().numpy()
     eng.check()
-    value = ws * n * args.steps / (total_ms * 1e-3)
-    interactions_per_step = float(stats[0]) / args.steps   # body-node interactions
-    forces_ms = stages.get("forces", 0.0) / args.steps
+    value = ws * n * steps_done / (total_ms * 1e-3)
+    args.steps_done = steps_done
+    launches = launches_per_step
 
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+            "steps": steps_done, "warmup": args.warmup, "ms_per_step": total_ms / steps_done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Zel'dovich ICs)", "config": config_dict(cfg, args),
-            "gpu_launches": int(launches),
-            "stages_ms": {k: v / args.steps for k, v in stages.items()}}
+            "gpu_launches": int(launches) * steps_done,
+            "gpu_launches_per_step": int(launches), "cuda_graph": bool(args.graph),
+            "stages_ms_eager": stages}
+    if tune_report is not None:
+        line["autotune"] = tune_report
+    line["max_node_stack"] = int(eng.tree_manager.workspace[2].item()) if eng.tree_manager.node_table is not None else None
     if args.force_mode == "grouped":
         line["interactions_per_body"] = interactions_per_step / n
 

@@ -67,13 +67,13 @@ SIGNATURES = {
     "cnb_pack_nodes": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p]),
     "cnb_build_tree_ranges": (_int, [_p, _p, _p, _p, _i64, _p]),
     "cnb_make_buckets": (_int, [_p, _p, _i64, _int, _p, _p]),
-    "cnb_forces_grouped": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _d, _d, _d, _d,
-                                  _p, _p, _p]),
+    "cnb_forces_grouped": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _int, _d, _d, _d,
+                                  _d, _p, _p, _p]),
     "cnb_make_buckets_boxes": (_int, [_p, _p, _p, _int, _i64, _int, _p, _p]),
     "cnb_compute_codes_boxes": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
     "cnb_box_roots": (_int, [_p, _p, _p, _int, _i64, _int, _p, _p]),
     "cnb_forces_grouped_boxes": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p, _int, _p, _p, _p, _int, _int,
-                                        _d, _p, _p, _p]),
+                                        _int, _d, _p, _p, _p]),
     "cnb_integrate_boxes": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _int, _i64, _p, _p]),
     "cnb_bucket_features": (_int, [_p, _p, _p, _i64, _p, _int, _p]),
     "cnb_controller_theta": (_int, [_p, _p, _p, _i64, _p, _p, _int, _p]),

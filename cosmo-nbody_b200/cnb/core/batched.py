@@ -47,7 +47,8 @@ class BatchedBoxes:
     """Independent boxes in one tree.  `boxes` is a list of dicts with keys
     n_grid, seed, a_start, theta (see draw_boxes)."""
 
-    def __init__(self, boxes, mac="periodic", bodies_per_lane=1, da=0.002, G=1.0, H0=67.8,
+    def __init__(self, boxes, mac="periodic", bodies_per_lane=1, block_warps=4, da=0.002, G=1.0,
+                 H0=67.8,
                  omega_m=1.0, omega_l=0.692, slab_bodies=0.0, device=None):
         dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         self.device = dev
@@ -58,6 +59,7 @@ class BatchedBoxes:
             raise ValueError("too many boxes")
         self.mac = MACS[mac]
         self.bpl = int(bodies_per_lane)
+        self.block_warps = int(block_warps)
         self.da, self.G = float(da), float(G)
         self.H0, self.omega_m, self.omega_l = H0, omega_m, omega_l
         sizes = [b["n_grid"] ** 3 for b in boxes]
@@ -155,7 +157,7 @@ class BatchedBoxes:
                   self.table.data_ptr(), self.workspace.data_ptr(), self.force.data_ptr(), self.n,
                   self.codes_sorted.data_ptr(), self.box_bits, self.box_roots.data_ptr(),
                   self.box_params.data_ptr(), tpb.data_ptr() if tpb is not None else None, self.mac,
-                  self.bpl, self.G, self.stats.data_ptr(), status_buffer(self.device.index).data_ptr(), st)
+                  self.bpl, self.block_warps, self.G, self.stats.data_ptr(), status_buffer(self.device.index).data_ptr(), st)
 
     def integrate(self):
         """Per-box Hubble rate and time step on the device, then kick/drift and a += da."""

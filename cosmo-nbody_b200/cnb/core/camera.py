@@ -40,6 +40,22 @@ class Camera:
                   self.height, st)
         return self.grid_d
 
+    def mvp_host(self, step):
+        """The orbiting camera's MVP for `step` as a pinned host tensor."""
+        mvp = get_mvp_matrix(step, self.box_center, self.config.BOX_SIZE, self.config,
+                             aspect=self.width / self.height)
+        return torch.from_numpy(mvp).pin_memory()
+
+    def splat_device(self, mvp_d, px_d, py_d, pz_d):
+        """Clear and splat with an MVP already on the device (no host work, so
+        it can be captured in a CUDA graph)."""
+        self.grid_d.zero_()
+        st = int(torch.cuda.current_stream(self.device).cuda_stream)
+        _lib.call("cnb_render_density", px_d.data_ptr(), py_d.data_ptr(), pz_d.data_ptr(),
+                  self.grid_d.data_ptr(), mvp_d.data_ptr(), px_d.shape[0], self.width,
+                  self.height, st)
+        return self.grid_d
+
     def capture(self, step, px_d, py_d, pz_d):
         """camera.py:29-48: splat and colourise; returns the [H, W, 3] frame."""
         return colorize_frame(self.splat(step, px_d, py_d, pz_d))

@@ -36,6 +36,7 @@ class SimulationEngine:
         if self.force_mode not in ("reference", "grouped"):
             raise ValueError("FORCE_MODE must be 'reference' or 'grouped'")
         self.bodies_per_lane = int(getattr(config, "BODIES_PER_LANE", 1))
+        self.block_warps = int(getattr(config, "BLOCK_WARPS", 8))
         self.tree_manager = OctreeManager(state.n, config.TPB, device=state.device,
                                           upward=getattr(config, "UPWARD", "plain"),
                                           node_table=self.force_mode == "grouped",
@@ -80,7 +81,7 @@ class SimulationEngine:
             _lib.call("cnb_forces_grouped", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                       tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,
                       float(cfg.THETA), tpg.data_ptr() if tpg is not None else None, self.mac,
-                      self.bodies_per_lane, float(cfg.G), float(cfg.SOFTENING),
+                      self.bodies_per_lane, self.block_warps, float(cfg.G), float(cfg.SOFTENING),
                       float(cfg.BOX_SIZE), self.slab_mass, self.stats.data_ptr(), status, st)
         else:
             _lib.call("cnb_compute_forces", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
@@ -115,6 +116,53 @@ class SimulationEngine:
                   float(self.a), float(H), float(dt_physics), self._stream())
         self._mark("integrate")
         self.a += self.da
+
+    # ------------------------------------------------------------ CUDA graph
+    def _step_device(self, mvp=None):
+        """One step with no host scalars (a, H, dt live on the device), so it
+        can be captured; `mvp` (device [4,4]) also splats the new positions."""
+        self.forces_only()
+        a = self.a_dev
+        cfg = self.config
+        H = cfg.H0 * torch.sqrt(cfg.OMEGA_M * a ** -3 + cfg.OMEGA_L)
+        self.aHdt[:, 0] = a
+        self.aHdt[:, 1] = H
+        self.aHdt[:, 2] = self.da / (a * H) * 0.8
+        s = self.state
+        _lib.call("cnb_integrate_boxes", *(t.data_ptr() for t in s.pos + s.vel), s.force.data_ptr(),
+                  s.codes.data_ptr(), 0, s.n, self.aHdt.data_ptr(), self._stream())
+        self.a_dev += self.da
+        if mvp is not None and self.camera is not None:
+            self.camera.splat_device(mvp, *s.pos)
+
+    def capture(self, splat=True):
+        """Capture two consecutive steps (and their splats) in one CUDA graph.
+        The step alternates between two array sets, so after every replay the
+        arrays are back where they were captured.  Use replay() afterwards."""
+        self.a_dev = torch.tensor([self.a], dtype=torch.float64, device=self.state.device)
+        self.aHdt = torch.zeros((1, 3), dtype=torch.float64, device=self.state.device)
+        self.mvp_slots = torch.zeros((2, 4, 4), dtype=torch.float32, device=self.state.device)
+        self._graph_splat = bool(splat and self.camera is not None)
+        self._step_device(self.mvp_slots[0] if self._graph_splat else None)   # warm-up, eager
+        self._step_device(self.mvp_slots[1] if self._graph_splat else None)
+        self.a += 2 * self.da
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            for k in range(2):
+                self._step_device(self.mvp_slots[k] if self._graph_splat else None)
+        self._graph = g
+        self._graph_step = 2
+        return g
+
+    def replay(self):
+        """Two steps through the captured graph (camera orbit continues)."""
+        if self._graph_splat:
+            for k in range(2):
+                self.mvp_slots[k].copy_(self.camera.mvp_host(self._graph_step + k), non_blocking=True)
+        self._graph.replay()
+        self._graph_step += 2
+        self.a += 2 * self.da
 
     def enable_stage_timing(self, on=True):
         """Record CUDA events between the stages of every step (stage_times() reads them)."""

@@ -83,6 +83,14 @@ class OctreeManager:
                       self.bucket, self.workspace.data_ptr(), st)
         return self.root_idx
 
+    def rebucket(self, max_size):
+        """Rebuild the bucket table of the current tree with buckets of at most max_size bodies."""
+        self.bucket = int(max_size)
+        if self.node_table is not None and self.n > 0:
+            st = self._stream()
+            _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), self.n,
+                      self.bucket, self.workspace.data_ptr(), st)
+
     def get_buffers(self):
         """octree.py:85-93."""
         return {

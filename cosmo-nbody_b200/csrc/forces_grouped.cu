@@ -33,8 +33,7 @@
 
 namespace cnb {
 
-constexpr int kGWarps = 4;     // warps per block
-constexpr int kGStack = 2048;  // node stack entries per warp
+constexpr int kGStack = 1024;  // node stack entries per warp (deepest seen at 128^3: ~320)
 constexpr int kGList = 64;     // interaction list entries per warp
 
 struct GroupedParams {
@@ -90,14 +89,18 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
     }
 }
 
-template <int BPL>
-__global__ void __launch_bounds__(kGWarps * 32) k_forces_grouped(GroupedParams P) {
-    __shared__ int32_t s_stack[kGWarps][kGStack];
-    __shared__ float4 s_list[kGWarps][kGList];
+constexpr size_t grouped_smem(int warps) {
+    return (size_t)warps * (kGStack * sizeof(int32_t) + kGList * sizeof(float4));
+}
+
+template <int BPL, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) {
+    extern __shared__ __align__(16) unsigned char g_smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
-    int32_t *stack = s_stack[wib];
-    float4 *list = s_list[wib];
+    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * kGList;
+    int32_t *stack = reinterpret_cast<int32_t *>(g_smem + WARPS * kGList * sizeof(float4)) +
+                     wib * kGStack;
     unsigned long long n_tests = 0;
     int max_top = 0;
     bool overflow = false;
@@ -324,26 +327,40 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
     return launch_status();
 }
 
-static int launch_grouped(GroupedParams &P, int bodies_per_lane, cudaStream_t st) {
-    // persistent grid: the work counter hands out buckets
-    CNB_CUDA(cudaMemsetAsync(P.ws + 1, 0, 2 * sizeof(int32_t), st));
+template <int BPL, int WARPS>
+static int launch_shape(GroupedParams &P, cudaStream_t st) {
+    const size_t smem = grouped_smem(WARPS);
+    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    if (bodies_per_lane == 1) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<1>, kGWarps * 32, 0);
-        k_forces_grouped<1><<<kSMs * (per_sm > 0 ? per_sm : 1), kGWarps * 32, 0, st>>>(P);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<2>, kGWarps * 32, 0);
-        k_forces_grouped<2><<<kSMs * (per_sm > 0 ? per_sm : 1), kGWarps * 32, 0, st>>>(P);
-    }
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS>, WARPS * 32,
+                                                  smem);
+    // persistent grid: the work counter hands out buckets
+    k_forces_grouped<BPL, WARPS><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
     return launch_status();
+}
+
+static int launch_grouped(GroupedParams &P, int bodies_per_lane, int block_warps,
+                          cudaStream_t st) {
+    CNB_CUDA(cudaMemsetAsync(P.ws + 1, 0, 2 * sizeof(int32_t), st));
+    switch (bodies_per_lane * 16 + block_warps) {
+        case 16 + 2: return launch_shape<1, 2>(P, st);
+        case 16 + 4: return launch_shape<1, 4>(P, st);
+        case 16 + 8: return launch_shape<1, 8>(P, st);
+        case 32 + 2: return launch_shape<2, 2>(P, st);
+        case 32 + 4: return launch_shape<2, 4>(P, st);
+        case 32 + 8: return launch_shape<2, 8>(P, st);
+        default: return CNB_E_INVALID_ARG;
+    }
 }
 
 static int grouped_common(GroupedParams &P, const float *px, const float *py, const float *pz,
                           const float *node_table, int32_t *workspace, float *force, int64_t n,
-                          const float *theta_per_bucket, int mac, int bodies_per_lane, double G,
-                          unsigned long long *stats, int32_t *status) {
+                          const float *theta_per_bucket, int mac, int bodies_per_lane,
+                          int block_warps, double G, unsigned long long *stats, int32_t *status) {
     if (n < 0 || (mac != CNB_MAC_REF_X && mac != CNB_MAC_PERIODIC)) return CNB_E_INVALID_ARG;
     if (bodies_per_lane != 1 && bodies_per_lane != 2) return CNB_E_INVALID_ARG;
+    if (block_warps != 2 && block_warps != 4 && block_warps != 8) return CNB_E_INVALID_ARG;
     if (n == 0) return CNB_OK;
     if (!px || !py || !pz || !node_table || !force || !workspace) return CNB_E_INVALID_ARG;
     if ((reinterpret_cast<uintptr_t>(node_table) & 15) || (reinterpret_cast<uintptr_t>(workspace) & 15))
@@ -374,18 +391,18 @@ static int grouped_common(GroupedParams &P, const float *px, const float *py, co
 extern "C" int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                                   const float *node_table, int32_t *workspace, float *force,
                                   int64_t n, double theta, const float *theta_per_bucket,
-                                  int mac, int bodies_per_lane, double G, double soft, double box,
-                                  double slab_mass, unsigned long long *stats, int32_t *status,
-                                  void *stream) {
+                                  int mac, int bodies_per_lane, int block_warps, double G,
+                                  double soft, double box, double slab_mass,
+                                  unsigned long long *stats, int32_t *status, void *stream) {
     GroupedParams P;
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket, mac,
-                           bodies_per_lane, G, stats, status));
+                           bodies_per_lane, block_warps, G, stats, status));
     if (n == 0) return CNB_OK;
     P.theta = (float)theta;
     P.soft2 = (float)(soft * soft);
     P.box = (float)box;
     P.slab_mass = (float)slab_mass;
-    return launch_grouped(P, bodies_per_lane, as_stream(stream));
+    return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }
 
 extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,
@@ -393,12 +410,12 @@ extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const 
                                         int64_t n, const uint64_t *codes, int box_bits,
                                         const int32_t *box_roots, const float *box_params,
                                         const float *theta_per_bucket, int mac,
-                                        int bodies_per_lane, double G,
+                                        int bodies_per_lane, int block_warps, double G,
                                         unsigned long long *stats, int32_t *status,
                                         void *stream) {
     GroupedParams P;
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket, mac,
-                           bodies_per_lane, G, stats, status));
+                           bodies_per_lane, block_warps, G, stats, status));
     if (n == 0) return CNB_OK;
     if (!codes || !box_roots || !box_params || box_bits < 0 || box_bits > 30)
         return CNB_E_INVALID_ARG;
@@ -407,5 +424,5 @@ extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const 
     P.box_shift = 3 * ((63 - box_bits) / 3);
     P.box_roots = box_roots;
     P.box_params = reinterpret_cast<const float4 *>(box_params);
-    return launch_grouped(P, bodies_per_lane, as_stream(stream));
+    return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }

@@ -200,7 +200,8 @@ int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
  * interaction list, float32 with rsqrt, the minimum image per pair only
  * where a bucket's bodies can see different images.  theta_per_bucket
  * (device float per bucket slot, may be NULL) overrides theta.  mac:
- * CNB_MAC_REF_X or CNB_MAC_PERIODIC.  bodies_per_lane: 1 or 2.  slab_mass
+ * CNB_MAC_REF_X or CNB_MAC_PERIODIC.  bodies_per_lane: 1 or 2 (buckets of
+ * up to 32 or 64 bodies); block_warps: 2, 4 or 8 warps per block.  slab_mass
  * (CNB_MAC_PERIODIC only): nodes whose image differs between a bucket's
  * bodies are opened unless their mass is at most slab_mass, in which case
  * they are applied with the per-pair minimum image of their CoM (0 = exact
@@ -210,7 +211,7 @@ int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
 int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                        const float *node_table, int32_t *workspace, float *force, int64_t n,
                        double theta, const float *theta_per_bucket, int mac, int bodies_per_lane,
-                       double G, double soft, double box, double slab_mass,
+                       int block_warps, double G, double soft, double box, double slab_mass,
                        unsigned long long *stats, int32_t *status, void *stream);
 
 /* ---- many independent boxes in one launch (no reference counterpart) ----
@@ -233,7 +234,8 @@ int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,
                              const float *node_table, int32_t *workspace, float *force, int64_t n,
                              const uint64_t *codes, int box_bits, const int32_t *box_roots,
                              const float *box_params, const float *theta_per_bucket, int mac,
-                             int bodies_per_lane, double G, unsigned long long *stats,
+                             int bodies_per_lane, int block_warps, double G,
+                             unsigned long long *stats,
                              int32_t *status, void *stream);
 
 /* physics_kernels.py:155-203 integrate with per-box (a, H, dt): box_aHdt is

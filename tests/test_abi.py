@@ -46,9 +46,11 @@ def test_host_only_entry_points():
     assert lib.cnb_compute_codes(None, None, None, None, None, 0, 0, None) == _lib.CNB_OK
     assert lib.cnb_compute_codes(None, None, None, None, None, -1, 0, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_build_tree(None, None, None, 5, None) == _lib.CNB_E_INVALID_ARG
-    assert lib.cnb_forces_grouped(None, None, None, None, None, None, 5, 0.5, None, 7, 1, 1.0,
+    assert lib.cnb_forces_grouped(None, None, None, None, None, None, 5, 0.5, None, 7, 1, 4, 1.0,
                                   0.01, 1.0, 0.0, None, None, None) == _lib.CNB_E_INVALID_ARG
-    assert lib.cnb_forces_grouped(None, None, None, None, None, None, 5, 0.5, None, 0, 3, 1.0,
+    assert lib.cnb_forces_grouped(None, None, None, None, None, None, 5, 0.5, None, 0, 3, 4, 1.0,
+                                  0.01, 1.0, 0.0, None, None, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_forces_grouped(None, None, None, None, None, None, 5, 0.5, None, 0, 1, 3, 1.0,
                                   0.01, 1.0, 0.0, None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_make_buckets(None, None, 5, 32, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_sort_pairs(None, None, None, None, None, 5, 30, None) == _lib.CNB_E_INVALID_ARG

@@ -232,5 +232,50 @@ def test_bad_arguments_raise():
         build_tree[1, 256](codes.to(torch.int64), child, torch.zeros(19, dtype=torch.int32, device="cuda"))
     from cnb import _lib
     with pytest.raises(CnbError):
-        _lib.call("cnb_forces_grouped", 16, 16, 16, 16, 16, 16, 10, 0.5, None, 9, 1, 1.0, 0.1, 1.0,
-                  0.0, None, None, None)
+        _lib.call("cnb_forces_grouped", 16, 16, 16, 16, 16, 16, 10, 0.5, None, 9, 1, 4, 1.0, 0.1,
+                  1.0, 0.0, None, None, None)
+
+
+def test_engine_graph_replay_equals_device_steps():
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = config(16, KEY_MODE="morton63", FORCE_MODE="grouped", RES_W=96, RES_H=54)
+    pos, vel = zeldovich_arrays(16, 5)
+    eager = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel))
+    graphed = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel))
+    graphed.capture(splat=True)          # two eager warm-up steps, then a 2-step graph
+    eager.a_dev = torch.tensor([eager.a], dtype=torch.float64, device="cuda")
+    eager.aHdt = torch.zeros((1, 3), dtype=torch.float64, device="cuda")
+    mvp = torch.zeros((4, 4), device="cuda")
+    for k in range(6):
+        mvp.copy_(eager.camera.mvp_host(k))
+        eager._step_device(mvp)
+        if k >= 2 and k % 2 == 1:
+            graphed.replay()
+    torch.cuda.synchronize()
+    for a, b in zip(eager.state.pos + eager.state.vel, graphed.state.pos + graphed.state.vel):
+        np.testing.assert_array_equal(host(a), host(b))
+    # the splat adds float32 atomically: same pixels, sums equal up to addition order
+    ge, gg = host(eager.camera.grid_d), host(graphed.camera.grid_d)
+    np.testing.assert_array_equal(ge != 0, gg != 0)
+    np.testing.assert_allclose(ge, gg, rtol=1e-5, atol=0)
+    assert abs(graphed.a - float(host(graphed.a_dev)[0])) < 1e-12
+    graphed.check()
+
+
+def test_device_step_matches_host_step():
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = config(16, KEY_MODE="morton63", FORCE_MODE="grouped")
+    pos, vel = zeldovich_arrays(16, 6)
+    a_eng = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel), camera=False)
+    b_eng = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel), camera=False)
+    b_eng.a_dev = torch.tensor([b_eng.a], dtype=torch.float64, device="cuda")
+    b_eng.aHdt = torch.zeros((1, 3), dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        a_eng.step()
+        b_eng._step_device()
+    for a, b in zip(a_eng.state.pos + a_eng.state.vel, b_eng.state.pos + b_eng.state.vel):
+        np.testing.assert_allclose(host(a), host(b), rtol=1e-6, atol=1e-7)

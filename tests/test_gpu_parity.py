@@ -423,7 +423,7 @@ def test_direct_sum_gpu_matches_oracle():
     np.testing.assert_allclose(got, want, rtol=0, atol=1e-11 * np.abs(want).max())
 
 
-def grouped(pos, codes, mass, theta, soft, mac, tpg=None, bpl=1, want_ws=False, slab=0.0):
+def grouped(pos, codes, mass, theta, soft, mac, tpg=None, bpl=1, want_ws=False, slab=0.0, warps=4):
     """Tree (with node ranges), node table, buckets and the grouped traversal."""
     n = pos[0].size
     m = 2 * n - 1
@@ -450,8 +450,8 @@ def grouped(pos, codes, mass, theta, soft, mac, tpg=None, bpl=1, want_ws=False, 
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     T = dev(tpg.astype(np.float32)) if tpg is not None else None
     lib().call("cnb_forces_grouped", *(p.data_ptr() for p in P), table.data_ptr(), ws.data_ptr(),
-               F.data_ptr(), n, theta, T.data_ptr() if T is not None else None, mac, bpl, 1.0, soft,
-               1.0, slab, stats.data_ptr(), status.data_ptr(), stream())
+               F.data_ptr(), n, theta, T.data_ptr() if T is not None else None, mac, bpl, warps, 1.0,
+               soft, 1.0, slab, stats.data_ptr(), status.data_ptr(), stream())
     out = (host(F), host(stats), int(host(status)[0]))
     return out + (host(ws),) if want_ws else out
 
@@ -493,7 +493,7 @@ def test_buckets_partition_the_bodies(bpl):
     starts, counts = b[order, 0], b[order, 1]
     np.testing.assert_array_equal(starts[1:], (starts + counts)[:-1])
     assert starts[0] == 0 and starts[-1] + counts[-1] == n
-    assert 0 < ws[2] <= 2048   # deepest node stack
+    assert 0 < ws[2] <= 1024   # deepest node stack
 
 
 def test_grouped_ref_mac_accuracy_vs_reference_traversal():
