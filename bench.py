@@ -87,14 +87,25 @@ def dist_init():
     return ws, rank, local
 
 
-def max_over_ranks(x, ws):
+def replica_seed(rank):
+    """Seed of the independent box a rank simulates (replicas, weak scaling)."""
+    return 1 + 1000 * rank
+
+
+def max_over_ranks(x, ws, device="cuda"):
+    """The largest value of x over all ranks (the job's time is its slowest rank's)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_rate(bodies_per_rank, steps, ws, max_ms):
+    """Whole-job particle-steps/s: every rank's bodies x steps over the slowest rank's time."""
+    return ws * bodies_per_rank * steps / (max_ms * 1e-3)
 
 
 def barrier(ws):
@@ -276,7 +287,7 @@ def run_ours(args):
 
     ws, rank, local = dist_init()
     torch.cuda.set_device(local)
-    seed = 1 + 1000 * rank
+    seed = replica_seed(rank)
     cfg = make_config(args, seed)
     n = cfg.N_BODIES
     pos_h, vel_h = zeldovich_arrays(cfg.N_GRID, seed)
@@ -346,7 +357,7 @@ def run_ours(args):
     step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
     total_ms = max_over_ranks(sum(step_ms), ws)
     eng.check()
-    value = ws * n * steps_done / (total_ms * 1e-3)
+    value = aggregate_rate(n, steps_done, ws, total_ms)
     args.steps_done = steps_done
     launches = launches_per_step
 
@@ -359,6 +370,14 @@ def run_ours(args):
             "stages_ms_eager": stages}
     if tune_report is not None:
         line["autotune"] = tune_report
+    # HBM-bound stages against the measured copy bandwidth, algorithmic bytes per body:
+    # keys 20 + sort 20 + permute 60; build 20 + upward/normalise 190; integrate 60
+    hbm = measured_peaks()["hbm_gbs"]
+    algo = {"sort": 100, "tree": 210, "integrate": 60}
+    line["stage_roofline"] = {
+        k: {"ms": stages[k], "bytes_per_body": b, "GB/s": n * b / (stages[k] * 1e-3) / 1e9,
+            "frac_of_measured_hbm": n * b / (stages[k] * 1e-3) / 1e9 / hbm}
+        for k, b in algo.items() if stages.get(k)}
     line["max_node_stack"] = int(eng.tree_manager.workspace[2].item()) if eng.tree_manager.node_table is not None else None
     if args.force_mode == "grouped":
         line["interactions_per_body"] = interactions_per_step / n

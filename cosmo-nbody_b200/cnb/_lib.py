@@ -81,6 +81,7 @@ SIGNATURES = {
     "cnb_mlp_grad": (_int, [_p, _p, _int, _p, _f, _p, _p, _p, _p]),
     "cnb_adam_step": (_int, [_p, _p, _p, _p, _int, _f, _f, _f, _f, _int, _p]),
     "cnb_to_bf16": (_int, [_p, _p, _int, _p]),
+    "cnb_colorize": (_int, [_p, _int, _int, _p, _p, _p, _p]),
     "cnb_direct_sum_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_fma_probe": (_int, [_p, _i64, _int, _p]),
 }

@@ -1,0 +1,280 @@
+"""Measurement studies of the B200 step beyond the headline benchmark.
+
+    python -m cnb.studies precision   [--n-grid 256] [--steps 50]
+    python -m cnb.studies batched     [--boxes 64] [--steps 10]
+    python -m cnb.studies controller  [--n-grid 128] [--evolve 100]
+
+precision:  Zel'dovich n^3 (seed 2) evolved `steps` kick-drift steps from
+            a = 0.02 with da = 0.002; then, for theta in {0.3, 0.5, 0.7}, both
+            opening tests and both upward passes (plain / compensated float32
+            with float64 root), the forces against the float64 minimum-image
+            direct sum on a seeded 4 096-body sample, and the node mass / CoM
+            error of the upward pass against float64 sums.
+batched:    64 boxes, n drawn from {16, 24, 32, 48, 64}^3 (seed 3), a_start in
+            [0.02, 0.1], theta in [0.3, 0.8]: particle-steps/s of the batched
+            step (one persistent traversal launch, CUDA graph) against the
+            same boxes stepped one by one.
+controller: labels from the batched boxes, training on the GPU, and learned
+            theta against plain theta = 0.5 at matched 99th-percentile error
+            on an evolved n^3 state (seed 4).
+Each prints one JSON object per configuration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+import torch
+
+from . import _lib
+from .core.batched import BatchedBoxes, draw_boxes
+from .core.engine import SimulationEngine
+from .core.state import SimulationState
+from .utils import config as cfgmod
+from .utils.cosmology import density_contrast_sigma, zeldovich_arrays
+
+
+def _cfg(n_grid, **kw):
+    base = dict(N_GRID=n_grid, SOFTENING=0.5 / n_grid, THETA=0.5, KEY_MODE="morton63",
+                FORCE_MODE="grouped", MAC="ref_x", N_STEPS=1000, A_START=0.02,
+                A_END=0.02 + 1000 * 0.002)
+    base.update(kw)
+    return cfgmod.make(**base)
+
+
+def _evolve(n_grid, seed, steps):
+    """State after `steps` steps of the plain recipe (reference opening test)."""
+    pos, vel = zeldovich_arrays(n_grid, seed)
+    eng = SimulationEngine(_cfg(n_grid), SimulationState(n_grid ** 3, pos, vel), camera=False)
+    for _ in range(steps):
+        eng.step()
+    eng.check()
+    return [p.clone() for p in eng.state.pos], [v.clone() for v in eng.state.vel], eng.a
+
+
+def _direct(state, targets, soft):
+    T = torch.from_numpy(targets).cuda()
+    out = torch.empty((targets.size, 3), dtype=torch.float64, device="cuda")
+    _lib.call("cnb_direct_sum_f64", *(p.data_ptr() for p in state.pos), state.mass.data_ptr(), state.n,
+              T.data_ptr(), targets.size, 1.0, float(soft), out.data_ptr(),
+              int(torch.cuda.current_stream().cuda_stream))
+    return out
+
+
+def _errors(force, ref, targets):
+    got = force[torch.from_numpy(targets).cuda()].double()
+    e = (got - ref).norm(dim=1) / ref.norm(dim=1)
+    rms = ref.norm(dim=1).pow(2).mean().sqrt()
+    en = (got - ref).norm(dim=1) / rms
+    q = lambda t, p: float(torch.quantile(t, p).item())
+    return dict(median_rel=q(e, 0.5), p99_rel=q(e, 0.99), median_rms=q(en, 0.5), p99_rms=q(en, 0.99))
+
+
+def precision(args):
+    pos, vel, a = _evolve(args.n_grid, 2, args.steps)
+    n = args.n_grid ** 3
+    sigma = density_contrast_sigma(*(p.cpu().numpy() for p in pos))
+    targets = None
+    ref = None
+    for upward in ("plain", "compensated"):
+        for mac in ("ref_x", "periodic"):
+            for theta in (0.3, 0.5, 0.7):
+                cfg = _cfg(args.n_grid, THETA=theta, MAC=mac, UPWARD=upward)
+                st = SimulationState(n, pos, vel)
+                eng = SimulationEngine(cfg, st, camera=False)
+                eng.forces_only()
+                eng.stats.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                eng.compute_forces()
+                e1.record()
+                torch.cuda.synchronize()
+                eng.check()
+                if targets is None:
+                    targets = np.sort(np.random.default_rng(0).choice(n, 4096, replace=False)).astype(np.int64)
+                    ref = _direct(st, targets, cfg.SOFTENING)
+                out = dict(study="precision", n_grid=args.n_grid, a=a, steps=args.steps,
+                           sigma_delta_64=sigma, upward=upward, mac=mac, theta=theta,
+                           forces_ms=e0.elapsed_time(e1),
+                           interactions_per_body=float(eng.stats[0].item()) / n,
+                           **_errors(st.force, ref, targets))
+                if upward == "compensated":
+                    r = eng.tree_manager.root_f64.cpu().numpy()
+                    out["root_mass_f64"] = float(r[0])
+                out["root_mass_f32"] = float(eng.tree_manager.mass[n].item())
+                print(json.dumps(out), flush=True)
+    # upward-pass error against float64 sums on a sample of internal nodes
+    st = SimulationState(n, pos, vel)
+    st.sort_buffer_by_morton(_cfg(args.n_grid))
+    for upward in ("plain", "compensated"):
+        eng = SimulationEngine(_cfg(args.n_grid, UPWARD=upward), st, camera=False)
+        eng.tree_manager.build(st.pos, st.mass, st.codes)
+        tm = eng.tree_manager
+        # float64 reference for a sample of internal nodes by prefix sums over the sorted bodies
+        m64 = st.mass.double()
+        cs = [torch.cumsum(m64 * p.double(), 0) for p in st.pos]
+        cm = torch.cumsum(m64, 0)
+        nodes = torch.arange(n, 2 * n - 1, max(1, n // 4096), device="cuda")
+        lo_hi = _node_ranges(tm, nodes)
+        lo, hi = lo_hi[:, 0], lo_hi[:, 1]
+        def seg(c):
+            return c[hi] - torch.where(lo > 0, c[(lo - 1).clamp_min(0)], torch.zeros_like(c[hi]))
+        mref = seg(cm)
+        cref = torch.stack([seg(c) / mref for c in cs], 1)
+        merr = ((tm.mass[nodes].double() - mref).abs() / mref).max().item()
+        cerr = (tm.com[nodes].double() - cref).abs().max().item()
+        print(json.dumps(dict(study="upward", n_grid=args.n_grid, upward=upward,
+                              max_rel_mass_err=merr, max_abs_com_err=cerr,
+                              nodes_checked=int(nodes.numel()))), flush=True)
+
+
+def _node_ranges(tm, nodes):
+    """Body range [lo, hi] of internal nodes (from a leftmost / rightmost descent)."""
+    ch = tm.child
+    n = tm.n
+    lo = nodes.clone()
+    hi = nodes.clone()
+    for _ in range(200):
+        l_int = lo >= n
+        h_int = hi >= n
+        if not bool(l_int.any() or h_int.any()):
+            break
+        lo = torch.where(l_int, ch[lo.clamp_max(ch.shape[0] - 1), 0].long(), lo)
+        hi = torch.where(h_int, ch[hi.clamp_max(ch.shape[0] - 1), 1].long(), hi)
+    return torch.stack([lo, hi], 1)
+
+
+def batched(args):
+    boxes = draw_boxes(args.boxes, seed=3)
+    bb = BatchedBoxes(boxes, mac=args.mac)
+    n = bb.n
+    from .autotune import SHAPES
+    # launch shape for this workload
+    bb.sort_and_build()
+    best = None
+    for bpl, warps in SHAPES:
+        bb.bpl, bb.block_warps = bpl, warps
+        bb.sort_and_build()
+        bb.compute_forces()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        bb.compute_forces()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if best is None or ms < best[0]:
+            best = (ms, bpl, warps)
+    bb.bpl, bb.block_warps = best[1], best[2]
+    bb.capture(warmup=1)
+    steps = args.steps + (args.steps % 2)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps // 2):
+        bb.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    bb.check()
+    batched_ms = e0.elapsed_time(e1) / steps
+    # the same boxes one after another through the single-box engine
+    seq_ms = 0.0
+    for d in boxes:
+        cfg = _cfg(d["n_grid"], THETA=d["theta"], MAC=args.mac, A_START=d["a_start"],
+                   BODIES_PER_LANE=best[1], BLOCK_WARPS=best[2])
+        pos, vel = zeldovich_arrays(d["n_grid"], d["seed"], d["a_start"])
+        eng = SimulationEngine(cfg, SimulationState(d["n_grid"] ** 3, pos, vel), camera=False)
+        eng.step()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record()
+        for _ in range(2):
+            eng.step()
+        t1.record()
+        torch.cuda.synchronize()
+        seq_ms += t0.elapsed_time(t1) / 2
+    print(json.dumps(dict(study="batched", boxes=args.boxes, bodies=n, mac=args.mac,
+                          shape=dict(bodies_per_lane=best[1], block_warps=best[2]),
+                          batched_ms_per_step=batched_ms,
+                          batched_particle_steps_per_s=n / (batched_ms * 1e-3),
+                          sequential_ms_per_step=seq_ms,
+                          sequential_particle_steps_per_s=n / (seq_ms * 1e-3),
+                          speedup=seq_ms / batched_ms)), flush=True)
+
+
+def controller(args):
+    from .controller import ThetaController, make_labels
+    t0 = time.time()
+    train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac="periodic")
+    X, y, info = make_labels(train, per_box=args.per_box, error=args.error)
+    del train
+    ctl = ThetaController(seed=0)
+    curve = ctl.train(X, y, steps=args.train_steps, lr=3e-3, over_weight=4.0)
+    pos, vel, a = _evolve(args.n_grid, 4, args.evolve)
+    n = args.n_grid ** 3
+    cfg = _cfg(args.n_grid, MAC="periodic")
+    st = SimulationState(n, pos, vel)
+    eng = SimulationEngine(cfg, st, camera=False)
+    eng.forces_only()
+    targets = np.sort(np.random.default_rng(0).choice(n, 4096, replace=False)).astype(np.int64)
+    ref = _direct(st, targets, cfg.SOFTENING)
+    key = "p99_rms" if args.error == "rms" else "p99_rel"
+
+    def run(scale=None):
+        eng.controller = ctl if scale is not None else None
+        eng.controller_scale = scale or 1.0
+        if scale is None:
+            eng.theta_per_group = None
+        eng.stats.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.compute_forces()
+        e1.record()
+        torch.cuda.synchronize()
+        s = eng.stats.cpu().numpy()
+        return dict(_errors(st.force, ref, targets), ms=e0.elapsed_time(e1),
+                    interactions=float(s[0]) / n, theta_dependent=float(s[0] - s[2]) / n)
+
+    plain = run(None)
+    lo, hi = 0.3, 3.0
+    for _ in range(12):
+        mid = 0.5 * (lo + hi)
+        r = run(mid)
+        lo, hi = (mid, hi) if r[key] <= plain[key] else (lo, mid)
+    learned = run(lo)
+    eng.controller = None
+    eng.check()
+    print(json.dumps(dict(study="controller", n_grid=args.n_grid, evolve_steps=args.evolve, a=a,
+                          error=args.error, labels=info, train_loss=[curve[0], curve[-1]],
+                          plain_theta05=plain, learned=learned, learned_scale=lo,
+                          speedup_forces=plain["ms"] / learned["ms"],
+                          seconds=time.time() - t0)), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("study", choices=["precision", "batched", "controller"])
+    ap.add_argument("--n-grid", type=int, default=None)
+    ap.add_argument("--steps", type=int, default=None)
+    ap.add_argument("--boxes", type=int, default=64)
+    ap.add_argument("--mac", default="periodic")
+    ap.add_argument("--evolve", type=int, default=100)
+    ap.add_argument("--per-box", type=int, default=48)
+    ap.add_argument("--train-steps", type=int, default=1500)
+    ap.add_argument("--error", default="rms", choices=["rms", "relative"])
+    args = ap.parse_args()
+    if args.study == "precision":
+        args.n_grid = args.n_grid or 256
+        args.steps = 50 if args.steps is None else args.steps
+        precision(args)
+    elif args.study == "batched":
+        args.steps = args.steps or 10
+        batched(args)
+    else:
+        args.n_grid = args.n_grid or 128
+        controller(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -61,7 +61,17 @@ struct GroupedParams {
     int32_t *status;
 };
 
-template <int BPL>
+// Nearest-image offset of a coordinate difference d with |d| < 1.5:
+// -1, 0 or +1, equal to rint(d) there (ties at +-0.5 round to 0, as rint
+// does); compare-and-select keeps it on the FP32 pipe.
+__device__ __forceinline__ float image_of(float d) {
+    return d > 0.5f ? 1.f : (d < -0.5f ? -1.f : 0.f);
+}
+
+// Applies cnt list entries (x, y, z, mass) to the lane's BPL bodies.  WRAP:
+// the entries' image may differ between the bucket's bodies, so every pair
+// takes its own minimum image.
+template <int BPL, bool WRAP>
 __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const float (&x)[BPL],
                                            const float (&y)[BPL], const float (&z)[BPL],
                                            float soft2, float (&ax)[BPL], float (&ay)[BPL],
@@ -69,19 +79,17 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
 #pragma unroll 4
     for (int j = 0; j < cnt; ++j) {
         const float4 e = list[j];
-        const bool wrap = e.w < 0.f;  // same entry in every lane: uniform branch
-        const float m = fabsf(e.w);
 #pragma unroll
         for (int b = 0; b < BPL; ++b) {
             float dx = e.x - x[b], dy = e.y - y[b], dz = e.z - z[b];
-            if (wrap) {
-                dx -= rintf(dx);
-                dy -= rintf(dy);
-                dz -= rintf(dz);
+            if (WRAP) {
+                dx -= image_of(dx);
+                dy -= image_of(dy);
+                dz -= image_of(dz);
             }
             const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
             const float r = rsqrtf(d2 + soft2);
-            const float f = (d2 > 1e-7f) ? m * r * r * r : 0.f;
+            const float f = (d2 > 1e-7f) ? e.w * r * r * r : 0.f;
             ax[b] = fmaf(f, dx, ax[b]);
             ay[b] = fmaf(f, dy, ay[b]);
             az[b] = fmaf(f, dz, az[b]);
@@ -90,7 +98,7 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
 }
 
 constexpr size_t grouped_smem(int warps) {
-    return (size_t)warps * (kGStack * sizeof(int32_t) + kGList * sizeof(float4));
+    return (size_t)warps * (kGStack * sizeof(int32_t) + 2 * kGList * sizeof(float4));
 }
 
 template <int BPL, int WARPS>
@@ -98,8 +106,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
     extern __shared__ __align__(16) unsigned char g_smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
-    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * kGList;
-    int32_t *stack = reinterpret_cast<int32_t *>(g_smem + WARPS * kGList * sizeof(float4)) +
+    // two interaction lists per warp: entries with one image for the whole
+    // bucket, and entries needing the per-pair image
+    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * 2 * kGList;
+    float4 *wlist = list + kGList;
+    int32_t *stack = reinterpret_cast<int32_t *>(g_smem + WARPS * 2 * kGList * sizeof(float4)) +
                      wib * kGStack;
     unsigned long long n_tests = 0;
     int max_top = 0;
@@ -162,7 +173,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
         float ax[BPL], ay[BPL], az[BPL];
 #pragma unroll
         for (int b = 0; b < BPL; ++b) ax[b] = ay[b] = az[b] = 0.f;
-        int top = 1, cnt = 0;
+        int top = 1, cnt = 0, wcnt = 0;
         unsigned long long n_entries = 0, n_wrap = 0;
         if (lane == 0) stack[0] = root;
         __syncwarp();
@@ -193,7 +204,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                     c0 = __float_as_int(S.z);
                     c1 = __float_as_int(S.w);
                     float dx = A.x - gcx, dy = A.y - gcy, dz = A.z - gcz;
-                    const float sx_ = rintf(dx), sy_ = rintf(dy), sz_ = rintf(dz);
+                    const float sx_ = image_of(dx), sy_ = image_of(dy), sz_ = image_of(dz);
                     dx -= sx_;
                     dy -= sy_;
                     dz -= sz_;
@@ -230,10 +241,18 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             }
             n_tests += (node >= 0);
             const uint32_t am = __ballot_sync(0xffffffffu, accept);
-            n_wrap += __popc(__ballot_sync(0xffffffffu, accept && E.w < 0.f));
             const uint32_t om = __ballot_sync(0xffffffffu, open);
-            if (accept) list[cnt + __popc(am & lt)] = E;
-            cnt += __popc(am);
+            const bool to_w = accept && E.w < 0.f;
+            const uint32_t wm = __ballot_sync(0xffffffffu, to_w);
+            const uint32_t nm = am & ~wm;
+            if (accept) {
+                if (to_w)
+                    wlist[wcnt + __popc(wm & lt)] = make_float4(E.x, E.y, E.z, -E.w);
+                else
+                    list[cnt + __popc(nm & lt)] = E;
+            }
+            cnt += __popc(nm);
+            wcnt += __popc(wm);
             const int nopen = __popc(om);
             if (top + 2 * nopen > kGStack) {
                 overflow = true;  // children dropped (flagged)
@@ -248,16 +267,27 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             }
             __syncwarp();
             if (cnt >= 32) {
-                apply_list<BPL>(list, 32, x, y, z, soft2, ax, ay, az);
+                apply_list<BPL, false>(list, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 __syncwarp();
                 if (lane < cnt - 32) list[lane] = list[32 + lane];
                 cnt -= 32;
                 __syncwarp();
             }
+            if (wcnt >= 32) {
+                apply_list<BPL, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
+                n_entries += 32;
+                n_wrap += 32;
+                __syncwarp();
+                if (lane < wcnt - 32) wlist[lane] = wlist[32 + lane];
+                wcnt -= 32;
+                __syncwarp();
+            }
         }
-        apply_list<BPL>(list, cnt, x, y, z, soft2, ax, ay, az);
-        n_entries += cnt;
+        apply_list<BPL, false>(list, cnt, x, y, z, soft2, ax, ay, az);
+        apply_list<BPL, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
+        n_entries += cnt + wcnt;
+        n_wrap += wcnt;
         __syncwarp();
 #pragma unroll
         for (int b = 0; b < BPL; ++b) {

@@ -214,6 +214,13 @@ int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                        int block_warps, double G, double soft, double box, double slab_mass,
                        unsigned long long *stats, int32_t *status, void *stream);
 
+/* src/utils/visualizer.py:115-171 colorize_frame (+ the 8-bit packing of
+ * src/core/engine.py:139): grid [height, width] float32 -> rgb float32
+ * [height, width, 3] and/or rgb8 uint8 [height, width, 3] (either may be
+ * NULL).  scratch: one device uint32 (the running maximum). */
+int cnb_colorize(const float *grid, int width, int height, float *rgb, unsigned char *rgb8,
+                 unsigned int *scratch, void *stream);
+
 /* ---- many independent boxes in one launch (no reference counterpart) ----
  * Keys carry the box id in their top bits: key = box << 3L | morton_L(x,y,z),
  * L = (63 - box_bits) / 3 bits per axis, coordinates in each box's own unit

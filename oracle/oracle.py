@@ -241,3 +241,30 @@ def run_reference_step(pos, vel, mass, a, da, theta, G, soft, box=1.0, key_mode=
                 parents=parents, n_mass=n_mass, n_com=n_com, n_min=n_min, n_max=n_max,
                 root=root, force=force, drops=drops, visits=visits, new_pos=new[:3],
                 new_vel=new[3:], a_next=a + da, H=H, dt=dt)
+
+
+def colorize(grid):
+    """src/utils/visualizer.py:115-171 colorize_frame in float32 numpy (the
+    reference runs it in CuPy, float32).  Returns (rgb float32 [H,W,3], rgb8)."""
+    g = np.asarray(grid, np.float32)
+    img = np.log1p(g * np.float32(120.0))
+    img = img / (img.max() + np.float32(1e-9))
+    val = np.power(img, np.float32(2.2)).astype(np.float32)
+    T1, T2, T3 = np.float32(0.6), np.float32(0.72), np.float32(0.82)
+    r, gg, b = (np.zeros_like(val) for _ in range(3))
+    m1 = val <= T1
+    b[m1] = val[m1] / T1 * np.float32(0.8)
+    m2 = (val > T1) & (val <= T2)
+    t = (val[m2] - T1) / (T2 - T1)
+    b[m2] = (1 - t) * np.float32(0.8)
+    gg[m2] = t * np.float32(0.9)
+    m3 = (val > T2) & (val <= T3)
+    t = (val[m3] - T2) / (T3 - T2)
+    gg[m3] = np.float32(0.9) + t * np.float32(0.1)
+    r[m3] = t
+    m4 = val > T3
+    t = (val[m4] - T3) / (1 - T3)
+    r[m4] = 1
+    gg[m4] = 1 - t
+    frame = np.clip(np.stack([r, gg, b], axis=-1) * np.float32(1.3), 0, 1).astype(np.float32)
+    return frame, (frame * 255).astype(np.uint8)
