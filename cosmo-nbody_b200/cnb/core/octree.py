@@ -44,6 +44,7 @@ class OctreeManager:
         self.upward = upward
         self.err = torch.zeros((m, 4), dtype=torch.float32, device=dev) if upward == "compensated" else None
         self.root_f64 = torch.zeros(4, dtype=torch.float64, device=dev)
+        self._com_raw = False   # True after the fused pass: com holds mass-weighted sums
         self.node_table = None
         if node_table:
             # traversal records and boxes, node ranges and the bucket table
@@ -68,6 +69,18 @@ class OctreeManager:
         else:
             _lib.call("cnb_build_tree", codes_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(), n, st)
         px, py, pz = pos_d
+        if self.node_table is not None and self.upward == "plain":
+            # one pass: sums, boxes and the traversal table; com stays raw until asked for
+            _lib.call("cnb_upward_table", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                      mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
+                      self.mass.data_ptr(), self.com.data_ptr(), self.aabb_min.data_ptr(),
+                      self.aabb_max.data_ptr(), self.counters.data_ptr(), self.node_table.data_ptr(),
+                      n, status, st)
+            self._com_raw = True
+            _lib.call("cnb_find_root", self.parent.data_ptr(), self.root_idx.data_ptr(), m, st)
+            _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), n,
+                      self.bucket, self.workspace.data_ptr(), st)
+            return self.root_idx
         mode = _lib.UPWARD_COMPENSATED if self.upward == "compensated" else _lib.UPWARD_PLAIN
         _lib.call("cnb_upward", px.data_ptr(), py.data_ptr(), pz.data_ptr(), mass_d.data_ptr(),
                   self.child.data_ptr(), self.parent.data_ptr(), self.mass.data_ptr(),
@@ -92,7 +105,11 @@ class OctreeManager:
                       self.bucket, self.workspace.data_ptr(), st)
 
     def get_buffers(self):
-        """octree.py:85-93."""
+        """octree.py:85-93 (the CoM is normalised here if the fused pass left it raw)."""
+        if self._com_raw:
+            _lib.call("cnb_normalize_com", self.mass.data_ptr(), self.com.data_ptr(), self.n_nodes,
+                      self._stream())
+            self._com_raw = False
         return {
             "child": self.child,
             "mass": self.mass,

@@ -124,7 +124,7 @@ def precision(args):
         mref = seg(cm)
         cref = torch.stack([seg(c) / mref for c in cs], 1)
         merr = ((tm.mass[nodes].double() - mref).abs() / mref).max().item()
-        cerr = (tm.com[nodes].double() - cref).abs().max().item()
+        cerr = (tm.get_buffers()["com"][nodes].double() - cref).abs().max().item()
         print(json.dumps(dict(study="upward", n_grid=args.n_grid, upward=upward,
                               max_rel_mass_err=merr, max_abs_com_err=cerr,
                               nodes_checked=int(nodes.numel()))), flush=True)

@@ -129,6 +129,16 @@ int cnb_upward(const float *px, const float *py, const float *pz, const float *m
                float *n_min, float *n_max, float *n_err, int32_t *counts, int64_t n, int mode,
                double *root_f64, int32_t *status, void *stream);
 
+/* tree_kernels.py:131-191 compute_multipoles (plain, bit-exact sums) that
+ * also writes the node table of cnb_pack_nodes for every node as it is
+ * formed, with the normalised CoM of tree_kernels.py:193-214 -- one pass
+ * instead of upward + normalize + pack.  n_com keeps the raw mass-weighted
+ * sums (run cnb_normalize_com on them for the reference layout). */
+int cnb_upward_table(const float *px, const float *py, const float *pz, const float *mass,
+                     const int32_t *children, const int32_t *parents, float *n_mass,
+                     float *n_com, float *n_min, float *n_max, int32_t *counts,
+                     float *node_table, int64_t n, int32_t *status, void *stream);
+
 /* src/kernels/tree_kernels.py:193-214 normalize_com(n_mass, n_com, n_nodes). */
 int cnb_normalize_com(const float *n_mass, float *n_com, int64_t n_nodes, void *stream);
 

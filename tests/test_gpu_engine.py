@@ -136,7 +136,7 @@ def test_engine_step_matches_oracle(force_mode, precision):
     # tree stages are bit-exact in every mode
     np.testing.assert_array_equal(host(st.codes), want["codes"])
     np.testing.assert_array_equal(host(eng.tree_manager.child), want["children"])
-    np.testing.assert_array_equal(host(eng.tree_manager.com), want["n_com"])
+    np.testing.assert_array_equal(host(eng.tree_manager.get_buffers()["com"]), want["n_com"])
     f = host(st.force)
     scale = np.abs(want["force"]).max()
     err = np.abs(f - want["force"]).max(axis=1) / scale

@@ -1,0 +1,78 @@
+"""The fused upward pass (sums + traversal table in one kernel) writes the same
+bits as the separate upward, normalisation and packing kernels."""
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def _tree(n_grid, seed):
+    from cnb.utils.cosmology import zeldovich_arrays
+    (x, y, z), _ = zeldovich_arrays(n_grid, seed)
+    codes, _ = orc.compute_codes(x, y, z, 1)
+    perm = orc.argsort_stable(codes)
+    return [a[perm] for a in (x, y, z)], codes[perm]
+
+
+@pytest.mark.parametrize("n_grid", [2, 16, 32])
+def test_fused_table_equals_separate_passes(n_grid):
+    from cnb import _lib
+    pos, codes = _tree(n_grid, 3)
+    n = codes.size
+    m = 2 * n - 1
+    st = int(torch.cuda.current_stream().cuda_stream)
+    K = torch.from_numpy(codes).cuda()
+    P = [torch.from_numpy(a).cuda() for a in pos]
+    M = torch.full((n,), 1.0 / n, device="cuda")
+    ch = torch.full((m, 2), -1, dtype=torch.int32, device="cuda")
+    par = torch.full((m,), -1, dtype=torch.int32, device="cuda")
+    _lib.call("cnb_build_tree", K.data_ptr(), ch.data_ptr(), par.data_ptr(), n, st)
+
+    def bufs():
+        return [torch.zeros(m, device="cuda"), torch.zeros((m, 3), device="cuda"),
+                torch.zeros((m, 3), device="cuda"), torch.zeros((m, 3), device="cuda"),
+                torch.zeros(m, dtype=torch.int32, device="cuda")]
+
+    a = bufs()
+    _lib.call("cnb_upward", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(), par.data_ptr(),
+              *(t.data_ptr() for t in a[:4]), None, a[4].data_ptr(), n, 0, None, None, st)
+    table_a = torch.empty((4, m, 4), device="cuda")
+    _lib.call("cnb_pack_nodes", *(t.data_ptr() for t in a[:4]), ch.data_ptr(), table_a.data_ptr(), m, st)
+    b = bufs()
+    table_b = torch.empty((4, m, 4), device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    _lib.call("cnb_upward_table", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(), par.data_ptr(),
+              *(t.data_ptr() for t in b[:4]), b[4].data_ptr(), table_b.data_ptr(), n, status.data_ptr(), st)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    np.testing.assert_array_equal(table_a.cpu().numpy().view(np.uint32), table_b.cpu().numpy().view(np.uint32))
+    # the fused pass leaves raw sums in n_com; normalising them gives the reference's values
+    _lib.call("cnb_normalize_com", b[0].data_ptr(), b[1].data_ptr(), m, st)
+    wm, wc, wlo, whi = orc.compute_multipoles(*pos, M.cpu().numpy(), ch.cpu().numpy(), par.cpu().numpy())
+    np.testing.assert_array_equal(b[1].cpu().numpy(), wc)
+    np.testing.assert_array_equal(b[0].cpu().numpy(), wm)
+
+
+def test_octree_manager_grouped_buffers_are_reference_layout():
+    from cnb.core.octree import OctreeManager
+    pos, codes = _tree(16, 4)
+    n = codes.size
+    P = [torch.from_numpy(a).cuda() for a in pos]
+    M = torch.full((n,), 1.0 / n, device="cuda")
+    tm = OctreeManager(n, node_table=True)
+    tm.build(P, M, torch.from_numpy(codes).cuda())
+    buf = tm.get_buffers()
+    ch, par = orc.build_tree(codes)
+    wm, wc, wlo, whi = orc.compute_multipoles(*pos, M.cpu().numpy(), ch, par)
+    np.testing.assert_array_equal(buf["com"].cpu().numpy(), wc)
+    np.testing.assert_array_equal(buf["min"].cpu().numpy(), wlo)
+    assert int(buf["root"].item()) == n
