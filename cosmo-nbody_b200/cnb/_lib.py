@@ -58,7 +58,8 @@ SIGNATURES = {
     "cnb_compute_multipoles": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_upward": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _int, _p, _p, _p]),
     "cnb_normalize_com": (_int, [_p, _p, _i64, _p]),
-    "cnb_upward_table": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
+    "cnb_upward_table": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
+    "cnb_unpack_nodes": (_int, [_p, _p, _p, _p, _p, _i64, _p]),
     "cnb_find_root": (_int, [_p, _p, _i64, _p]),
     "cnb_build_top_tree_cache": (_int, [_p, _p, _p, _p, _i32, _p]),
     "cnb_compute_forces": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _d, _d, _d, _d, _p, _i64,

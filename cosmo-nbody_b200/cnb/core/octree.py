@@ -44,11 +44,13 @@ class OctreeManager:
         self.upward = upward
         self.err = torch.zeros((m, 4), dtype=torch.float32, device=dev) if upward == "compensated" else None
         self.root_f64 = torch.zeros(4, dtype=torch.float64, device=dev)
-        self._com_raw = False   # True after the fused pass: com holds mass-weighted sums
+        # True after the fused pass: the reference-layout arrays are filled on demand
+        self._stale_ref = False
         self.node_table = None
         if node_table:
             # traversal records and boxes, node ranges and the bucket table
             self.node_table = torch.empty((4, m, 4), dtype=torch.float32, device=dev)
+            self.sums = torch.empty((m, 4), dtype=torch.float32, device=dev)   # climb scratch
             self.ranges = torch.zeros((max(self.n - 1, 1), 2), dtype=torch.int32, device=dev)
             self.workspace = torch.zeros(4 + 4 * max(self.n, 1), dtype=torch.int32, device=dev)
             self.bucket = int(bucket)
@@ -73,10 +75,9 @@ class OctreeManager:
             # one pass: sums, boxes and the traversal table; com stays raw until asked for
             _lib.call("cnb_upward_table", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                       mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
-                      self.mass.data_ptr(), self.com.data_ptr(), self.aabb_min.data_ptr(),
-                      self.aabb_max.data_ptr(), self.counters.data_ptr(), self.node_table.data_ptr(),
+                      self.counters.data_ptr(), self.node_table.data_ptr(), self.sums.data_ptr(),
                       n, status, st)
-            self._com_raw = True
+            self._stale_ref = True
             _lib.call("cnb_find_root", self.parent.data_ptr(), self.root_idx.data_ptr(), m, st)
             _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), n,
                       self.bucket, self.workspace.data_ptr(), st)
@@ -105,11 +106,12 @@ class OctreeManager:
                       self.bucket, self.workspace.data_ptr(), st)
 
     def get_buffers(self):
-        """octree.py:85-93 (the CoM is normalised here if the fused pass left it raw)."""
-        if self._com_raw:
-            _lib.call("cnb_normalize_com", self.mass.data_ptr(), self.com.data_ptr(), self.n_nodes,
-                      self._stream())
-            self._com_raw = False
+        """octree.py:85-93 (filled from the node table if the fused pass built the tree)."""
+        if self._stale_ref:
+            _lib.call("cnb_unpack_nodes", self.node_table.data_ptr(), self.mass.data_ptr(),
+                      self.com.data_ptr(), self.aabb_min.data_ptr(), self.aabb_max.data_ptr(),
+                      self.n_nodes, self._stream())
+            self._stale_ref = False
         return {
             "child": self.child,
             "mass": self.mass,

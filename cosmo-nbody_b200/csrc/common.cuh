@@ -33,6 +33,20 @@ __device__ __forceinline__ void set_flag(int32_t *status, int32_t bit) {
     if (status) atomicOr(status, bit);
 }
 
+// Device-scope atomic add with acquire-release semantics: the caller's
+// earlier stores are visible to whoever observes the increment (release),
+// and stores that other threads released before their increments are
+// visible to the caller's later loads (acquire).  One instruction in place of
+// fence + atomicAdd + fence.
+__device__ __forceinline__ int32_t atomic_add_acq_rel(int32_t *addr, int32_t v) {
+    int32_t old;
+    asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], %2;"
+                 : "=r"(old)
+                 : "l"(addr), "r"(v)
+                 : "memory");
+    return old;
+}
+
 }  // namespace cnb
 
 #define CNB_TRY(expr)                   \

@@ -130,35 +130,13 @@ __device__ __forceinline__ float two_sum_err(float a, float b, float s) {
     return __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
-// Normalised CoM of tree_kernels.py:193-214: c * (1.0 / m) in float64.
-__device__ __forceinline__ float norm_com(float c, float m) {
-    return m > 0.f ? __double2float_rn(__dmul_rn((double)c, __ddiv_rn(1.0, (double)m))) : c;
-}
-
-// Traversal record of a node (TABLE mode): (normalised com, mass | x-extent,
-// 3-D extent, children) and its box, as k_pack_nodes would write them.
-__device__ __forceinline__ void write_record(float4 *rec, float4 *aabb, int64_t v, float m,
-                                             float cx, float cy, float cz, float lx, float ly,
-                                             float lz, float hx, float hy, float hz, int32_t c0,
-                                             int32_t c1) {
-    const float sx = hx - lx;
-    rec[2 * v] = make_float4(norm_com(cx, m), norm_com(cy, m), norm_com(cz, m), m);
-    rec[2 * v + 1] = make_float4(sx, fmaxf(sx, fmaxf(hy - ly, hz - lz)), __int_as_float(c0),
-                                 __int_as_float(c1));
-    aabb[2 * v] = make_float4(lx, ly, lz, 0.f);
-    aabb[2 * v + 1] = make_float4(hx, hy, hz, 0.f);
-}
-
 // tree_kernels.py:131-191 compute_multipoles.  One thread per leaf; the
 // second arrival at a node (atomic counter) forms it from its two children
-// as (left + right) and climbs on.  Fences: the leaf / node data are made
-// visible before the counter increment (release), and the sibling's data are
-// read through L2 after it (acquire).  No thread ever waits.  A climb longer
+// as (left + right) and climbs on.  The counter increment is an acq_rel
+// atomic: it releases the node's data and acquires the sibling's, which are
+// then read through L2.  No thread ever waits.  A climb longer
 // than the node count flags CNB_FLAG_BAD_TOPOLOGY and stops.
-// TABLE: also write every node's traversal record (cnb_upward_table), so the
-// separate normalisation and packing passes are not needed; n_com then keeps
-// the raw mass-weighted sums.
-template <bool COMP, bool TABLE = false>
+template <bool COMP>
 __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
                                                 const float *__restrict__ py,
                                                 const float *__restrict__ pz,
@@ -167,9 +145,7 @@ __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
                                                 const int32_t *__restrict__ parents,
                                                 float *n_mass, float *n_com, float *n_min,
                                                 float *n_max, float *n_err, int32_t *counts,
-                                                int64_t n, int32_t *status,
-                                                float4 *rec = nullptr, float4 *aabb = nullptr) {
-    static_assert(!(COMP && TABLE), "the fused table is written by the plain pass only");
+                                                int64_t n, int32_t *status) {
     const int64_t m_nodes = 2 * n - 1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -199,8 +175,6 @@ __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
             a.ez = __fmaf_rn(z, a.m, -a.cz);
             reinterpret_cast<float4 *>(n_err)[i] = make_float4(a.em, a.ex, a.ey, a.ez);
         }
-        if (TABLE)
-            write_record(rec, aabb, i, a.m, a.cx, a.cy, a.cz, x, y, z, x, y, z, -1, -1);
         int64_t curr = i;
         for (int64_t guard = 0;; ++guard) {
             if (guard > m_nodes) {
@@ -213,9 +187,8 @@ __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
                 set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
                 break;
             }
-            __threadfence();
-            if (atomicAdd(counts + p, 1) == 0) break;
-            __threadfence();
+            // release this node's data, acquire the sibling's: the first arrival stops
+            if (atomic_add_acq_rel(counts + p, 1) == 0) break;
             const int32_t l = children[2 * p], r = children[2 * p + 1];
             const bool mine_left = (l == curr);
             const int32_t s = mine_left ? r : l;
@@ -269,9 +242,6 @@ __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
             n_max[3 * p] = q.hx;
             n_max[3 * p + 1] = q.hy;
             n_max[3 * p + 2] = q.hz;
-            if (TABLE)
-                write_record(rec, aabb, p, q.m, q.cx, q.cy, q.cz, q.lx, q.ly, q.lz, q.hx, q.hy,
-                             q.hz, l, r);
             a = q;
             curr = p;
         }
@@ -553,22 +523,3 @@ extern "C" int cnb_build_top_tree_cache(const int32_t *child, const int32_t *roo
     return launch_status();
 }
 
-extern "C" int cnb_upward_table(const float *px, const float *py, const float *pz,
-                                const float *mass, const int32_t *children,
-                                const int32_t *parents, float *n_mass, float *n_com,
-                                float *n_min, float *n_max, int32_t *counts, float *node_table,
-                                int64_t n, int32_t *status, void *stream) {
-    if (n < 0) return CNB_E_INVALID_ARG;
-    if (n == 0) return CNB_OK;
-    if (!px || !py || !pz || !mass || !children || !parents || !n_mass || !n_com || !n_min ||
-        !n_max || !counts || !node_table)
-        return CNB_E_INVALID_ARG;
-    if (reinterpret_cast<uintptr_t>(node_table) & 15) return CNB_E_INVALID_ARG;
-    if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
-    const int64_t m = 2 * n - 1;
-    float4 *rec = reinterpret_cast<float4 *>(node_table);
-    k_upward<false, true><<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
-        px, py, pz, mass, children, parents, n_mass, n_com, n_min, n_max, nullptr, counts, n,
-        status, rec, rec + 2 * m);
-    return launch_status();
-}

@@ -129,15 +129,22 @@ int cnb_upward(const float *px, const float *py, const float *pz, const float *m
                float *n_min, float *n_max, float *n_err, int32_t *counts, int64_t n, int mode,
                double *root_f64, int32_t *status, void *stream);
 
-/* tree_kernels.py:131-191 compute_multipoles (plain, bit-exact sums) that
- * also writes the node table of cnb_pack_nodes for every node as it is
- * formed, with the normalised CoM of tree_kernels.py:193-214 -- one pass
- * instead of upward + normalize + pack.  n_com keeps the raw mass-weighted
- * sums (run cnb_normalize_com on them for the reference layout). */
+/* tree_kernels.py:131-214 compute_multipoles + normalize_com for the grouped
+ * traversal: one pass that forms every node (float32 left + right sums,
+ * Numba min/max, CoM normalised in float64 -- the reference's arithmetic)
+ * and writes its record into node_table (the layout of cnb_pack_nodes,
+ * bit-identical to cnb_upward + cnb_pack_nodes).  sums: scratch float32
+ * [n_nodes, 4], 16-byte aligned (raw mass-weighted sums).  counts must be
+ * zero on entry.  The reference-layout arrays are not written; get them
+ * with cnb_unpack_nodes. */
 int cnb_upward_table(const float *px, const float *py, const float *pz, const float *mass,
-                     const int32_t *children, const int32_t *parents, float *n_mass,
-                     float *n_com, float *n_min, float *n_max, int32_t *counts,
-                     float *node_table, int64_t n, int32_t *status, void *stream);
+                     const int32_t *children, const int32_t *parents, int32_t *counts,
+                     float *node_table, float *sums, int64_t n, int32_t *status, void *stream);
+
+/* Reference-layout n_mass, n_com (normalised), n_min, n_max from a node table
+ * (src/core/octree.py:85-93 get_buffers). */
+int cnb_unpack_nodes(const float *node_table, float *n_mass, float *n_com, float *n_min,
+                     float *n_max, int64_t n_nodes, void *stream);
 
 /* src/kernels/tree_kernels.py:193-214 normalize_com(n_mass, n_com, n_nodes). */
 int cnb_normalize_com(const float *n_mass, float *n_com, int64_t n_nodes, void *stream);

@@ -49,17 +49,20 @@ def test_fused_table_equals_separate_passes(n_grid):
     _lib.call("cnb_pack_nodes", *(t.data_ptr() for t in a[:4]), ch.data_ptr(), table_a.data_ptr(), m, st)
     b = bufs()
     table_b = torch.empty((4, m, 4), device="cuda")
+    sums = torch.empty((m, 4), device="cuda")
     status = torch.zeros(1, dtype=torch.int32, device="cuda")
     _lib.call("cnb_upward_table", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(), par.data_ptr(),
-              *(t.data_ptr() for t in b[:4]), b[4].data_ptr(), table_b.data_ptr(), n, status.data_ptr(), st)
+              b[4].data_ptr(), table_b.data_ptr(), sums.data_ptr(), n, status.data_ptr(), st)
     torch.cuda.synchronize()
     assert int(status.item()) == 0
     np.testing.assert_array_equal(table_a.cpu().numpy().view(np.uint32), table_b.cpu().numpy().view(np.uint32))
-    # the fused pass leaves raw sums in n_com; normalising them gives the reference's values
-    _lib.call("cnb_normalize_com", b[0].data_ptr(), b[1].data_ptr(), m, st)
+    # the reference-layout arrays unpacked from the table are the reference's values
+    _lib.call("cnb_unpack_nodes", table_b.data_ptr(), *(t.data_ptr() for t in b[:4]), m, st)
     wm, wc, wlo, whi = orc.compute_multipoles(*pos, M.cpu().numpy(), ch.cpu().numpy(), par.cpu().numpy())
-    np.testing.assert_array_equal(b[1].cpu().numpy(), wc)
     np.testing.assert_array_equal(b[0].cpu().numpy(), wm)
+    np.testing.assert_array_equal(b[1].cpu().numpy(), wc)
+    np.testing.assert_array_equal(b[2].cpu().numpy(), wlo)
+    np.testing.assert_array_equal(b[3].cpu().numpy(), whi)
 
 
 def test_octree_manager_grouped_buffers_are_reference_layout():
