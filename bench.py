@@ -36,6 +36,9 @@ sys.path.insert(0, os.path.join(ROOT, "cosmo-nbody_b200"))
 METRIC = "particle-steps/s at N=128^3 (full plain step + 1920x1080 splat)"
 N_GRID = 128
 FLOPS_PER_INTERACTION = 20   # 3 sub, 3 min-image, 5 d2, 1 +eps2, 1 rsqrt, 3 mul, 3 fma (+1)
+# DRAM traffic of one k_forces_grouped launch on this workload, from the ncu capture
+# summarised in profiles/k_forces_grouped_128cube.md (dram__bytes_read.sum + write.sum)
+FORCES_TRAFFIC_BYTES_128 = 180.6e6 + 22.3e6
 
 
 def parse():
@@ -48,6 +51,8 @@ def parse():
     ap.add_argument("--theta", type=float, default=0.5)
     ap.add_argument("--force-mode", default="grouped", choices=["grouped", "reference"])
     ap.add_argument("--mac", default="ref_x", choices=["ref_x", "periodic"])
+    ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
+                    help="arithmetic of the reference force mode (f64 = the reference's)")
     ap.add_argument("--upward", default="plain", choices=["plain", "compensated"])
     ap.add_argument("--bpl", type=int, default=1, choices=[1, 2], help="bodies per lane (grouped)")
     ap.add_argument("--slab", type=float, default=0, help="periodic test: slab tolerance in bodies")
@@ -68,7 +73,7 @@ def make_config(args, seed):
     n = args.n_grid
     return cfgmod.make(N_GRID=n, SOFTENING=0.5 / n, THETA=args.theta, N_STEPS=10,
                        A_START=0.02, A_END=0.02 + 10 * 0.002, KEY_MODE="morton63",
-                       FORCE_MODE=args.force_mode, MAC=args.mac, PRECISION="f32",
+                       FORCE_MODE=args.force_mode, MAC=args.mac, PRECISION=args.precision,
                        UPWARD=args.upward, RES=args.width, RES_W=args.width, RES_H=args.height,
                        SEED=seed, BODIES_PER_LANE=args.bpl, SLAB_BODIES=args.slab)
 
@@ -272,6 +277,7 @@ def config_dict(cfg, args):
             "n_bodies": cfg.N_BODIES, "theta": cfg.THETA, "softening": cfg.SOFTENING,
             "da": 0.002, "a_start": cfg.A_START, "seed": 1, "keys": "morton63",
             "force_mode": cfg.FORCE_MODE, "mac": cfg.MAC, "upward": cfg.UPWARD,
+            "precision": cfg.PRECISION,
             "bodies_per_lane": cfg.BODIES_PER_LANE, "slab_bodies": cfg.SLAB_BODIES,
             "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}
 
@@ -387,7 +393,9 @@ def run_ours(args):
         achieved = interactions_per_step * FLOPS_PER_INTERACTION / (forces_ms * 1e-3) / 1e12
         line["roofline"] = {"kernel": "k_forces_grouped", "bound": "fp32", "achieved": achieved,
                             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                            "traffic": None,
+                            "traffic": FORCES_TRAFFIC_BYTES_128 if (args.n_grid == 128 and args.mac == "ref_x"
+                                                                    and abs(args.theta - 0.5) < 1e-9) else None,
+                            "traffic_unit": "bytes per launch (ncu capture, profiles/k_forces_grouped_128cube.md)",
                             "note": "peak = measured FP32 FMA throughput (cnb_fma_probe); "
                                     f"{FLOPS_PER_INTERACTION} flops per body-node interaction"}
         line["clocks"] = sampler.summary()
