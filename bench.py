@@ -36,9 +36,10 @@ sys.path.insert(0, os.path.join(ROOT, "cosmo-nbody_b200"))
 METRIC = "particle-steps/s at N=128^3 (full plain step + 1920x1080 splat)"
 N_GRID = 128
 FLOPS_PER_INTERACTION = 20   # 3 sub, 3 min-image, 5 d2, 1 +eps2, 1 rsqrt, 3 mul, 3 fma (+1)
-# DRAM traffic of one k_forces_grouped launch on this workload, from the ncu capture
-# summarised in profiles/k_forces_grouped_128cube.md (dram__bytes_read.sum + write.sum)
-FORCES_TRAFFIC_BYTES_128 = 180.6e6 + 22.3e6
+# DRAM traffic of one k_forces_grouped launch on this workload (64-body buckets, two-level
+# walk), from the ncu capture summarised in profiles/k_forces_grouped_128cube.md
+# (dram__bytes_read.sum + dram__bytes_write.sum)
+FORCES_TRAFFIC_BYTES_128 = 219.6e6 + 21.7e6
 
 
 def parse():
@@ -55,7 +56,11 @@ def parse():
                     help="arithmetic of the reference force mode (f64 = the reference's)")
     ap.add_argument("--upward", default="plain", choices=["plain", "compensated"])
     ap.add_argument("--bpl", type=int, default=1, choices=[1, 2], help="bodies per lane (grouped)")
+    ap.add_argument("--warps", type=int, default=8, choices=[2, 4, 8],
+                    help="warps per block of the grouped traversal (with --no-tune)")
     ap.add_argument("--slab", type=float, default=0, help="periodic test: slab tolerance in bodies")
+    ap.add_argument("--super", type=int, default=0,
+                    help="super-bucket size of the two-level walk (ref_x test; 0 = single level)")
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--accuracy-sample", type=int, default=4096)
@@ -75,7 +80,8 @@ def make_config(args, seed):
                        A_START=0.02, A_END=0.02 + 10 * 0.002, KEY_MODE="morton63",
                        FORCE_MODE=args.force_mode, MAC=args.mac, PRECISION=args.precision,
                        UPWARD=args.upward, RES=args.width, RES_W=args.width, RES_H=args.height,
-                       SEED=seed, BODIES_PER_LANE=args.bpl, SLAB_BODIES=args.slab)
+                       SEED=seed, BODIES_PER_LANE=args.bpl, SLAB_BODIES=args.slab,
+                       SUPER_BODIES=args.super, BLOCK_WARPS=args.warps)
 
 
 def dist_init():
@@ -376,6 +382,9 @@ def run_ours(args):
             "stages_ms_eager": stages}
     if tune_report is not None:
         line["autotune"] = tune_report
+    # the launch shape the timed steps used (the autotuner's choice, if it ran)
+    line["config"].update(bodies_per_lane=eng.bodies_per_lane, block_warps=eng.block_warps,
+                          super_bodies=eng.super_bodies)
     # HBM-bound stages against the measured copy bandwidth, algorithmic bytes per body:
     # keys 20 + sort 20 + permute 60; build 20 + upward/normalise 190; integrate 60
     hbm = measured_peaks()["hbm_gbs"]

@@ -58,6 +58,7 @@ SIGNATURES = {
     "cnb_compute_multipoles": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_upward": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _int, _p, _p, _p]),
     "cnb_normalize_com": (_int, [_p, _p, _i64, _p]),
+    "cnb_validate_tree": (_int, [_p, _p, _i64, _p, _p, _p]),
     "cnb_upward_table": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_unpack_nodes": (_int, [_p, _p, _p, _p, _p, _i64, _p]),
     "cnb_find_root": (_int, [_p, _p, _i64, _p]),
@@ -71,6 +72,9 @@ SIGNATURES = {
     "cnb_make_buckets": (_int, [_p, _p, _i64, _int, _p, _p]),
     "cnb_forces_grouped": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _int, _d, _d, _d,
                                   _d, _p, _p, _p]),
+    "cnb_two_level_workspace_bytes": (_i64, [_i64, _int]),
+    "cnb_forces_two_level": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _i64, _int, _p, _i64, _d, _int,
+                                    _int, _d, _d, _d, _p, _p, _p]),
     "cnb_make_buckets_boxes": (_int, [_p, _p, _p, _int, _i64, _int, _p, _p]),
     "cnb_compute_codes_boxes": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
     "cnb_box_roots": (_int, [_p, _p, _p, _int, _i64, _int, _p, _p]),

@@ -1,7 +1,8 @@
 """Autotuner for the grouped traversal's launch shape (no reference counterpart).
 
-Two knobs: bodies per lane (buckets of up to 32 or 64 bodies) and warps per
-block (2, 4 or 8).  `tune(engine)` times every shape on the engine's current
+Three knobs: bodies per lane (buckets of up to 32 or 64 bodies), warps per
+block (2, 4 or 8) and, with the reference opening test, the super-bucket size
+of the two-level walk (0 = single level).  `tune(engine)` times every shape on the engine's current
 tree with CUDA events and keeps the fastest; results are remembered per
 (GPU, opening test, theta, size class) in a JSON file next to this module so
 a later run on the same kind of GPU and workload can reuse them.
@@ -15,6 +16,7 @@ import os
 import torch
 
 SHAPES = ((1, 2), (1, 4), (1, 8), (2, 2), (2, 4), (2, 8))
+SUPERS = (0, 512, 1024)
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_tuned.json")
 
 
@@ -31,24 +33,28 @@ def _load():
         return {}
 
 
-def _apply(engine, bpl, warps):
+def _apply(engine, bpl, warps, super_bodies=0):
     engine.bodies_per_lane = bpl
     engine.block_warps = warps
     engine.tree_manager.rebucket(32 * bpl)
+    engine.set_super_bodies(super_bodies)
 
 
-def tune(engine, shapes=SHAPES, reps=3, use_cache=True, save=True):
-    """Pick the fastest (bodies_per_lane, block_warps) for `engine` (grouped
-    mode, tree already built by forces_only/step).  Returns a report dict."""
+def tune(engine, shapes=SHAPES, supers=SUPERS, reps=3, use_cache=True, save=True):
+    """Pick the fastest (bodies_per_lane, block_warps, super-bucket size) for
+    `engine` (grouped mode, tree already built by forces_only/step).  Returns
+    a report dict."""
     key = _key(engine)
+    if engine.mac != 0:          # the two-level walk exists for the reference test only
+        supers = (0,)
     cache = _load() if use_cache else {}
-    if key in cache:
-        bpl, warps = cache[key]["shape"]
-        _apply(engine, bpl, warps)
+    if key in cache and len(cache[key].get("shape", [])) == 3:
+        _apply(engine, *cache[key]["shape"])
         return dict(cache[key], cached=True)
     times = {}
-    for bpl, warps in shapes:
-        _apply(engine, bpl, warps)
+    configs = [(bpl, warps, sb) for bpl, warps in shapes for sb in supers]
+    for bpl, warps, sb in configs:
+        _apply(engine, bpl, warps, sb)
         engine.compute_forces()              # warm-up of this shape
         best = float("inf")
         for _ in range(reps):
@@ -58,10 +64,10 @@ def tune(engine, shapes=SHAPES, reps=3, use_cache=True, save=True):
             e1.record()
             e1.synchronize()
             best = min(best, e0.elapsed_time(e1))
-        times[f"{bpl}x{warps}"] = best
-    bpl, warps = min(shapes, key=lambda s: times[f"{s[0]}x{s[1]}"])
-    _apply(engine, bpl, warps)
-    report = {"shape": [bpl, warps], "ms": times}
+        times[f"{bpl}x{warps}s{sb}"] = best
+    bpl, warps, sb = min(configs, key=lambda c: times[f"{c[0]}x{c[1]}s{c[2]}"])
+    _apply(engine, bpl, warps, sb)
+    report = {"shape": [bpl, warps, sb], "ms": times}
     if save:
         cache = _load()
         cache[key] = report

@@ -11,7 +11,10 @@ kernel is chosen by config.FORCE_MODE:
                test (config.PRECISION "f64" = the reference's arithmetic,
                "f32" = float32);
   "grouped"    warp-per-bucket traversal (config.MAC "ref_x" or "periodic",
-               optional per-bucket theta from `theta_per_group`).
+               optional per-bucket theta from `theta_per_group`); with
+               config.SUPER_BODIES > 0 and the "ref_x" test, the two-level
+               form (super-buckets of that many bodies walk the top of the
+               tree once for all their buckets).
 
 Device error flags are read by `check()` (one synchronisation).
 """
@@ -59,8 +62,29 @@ class SimulationEngine:
         # periodic test: image-ambiguous nodes of at most SLAB_BODIES bodies' mass are applied
         # with the per-pair minimum image (0 = exact)
         self.slab_mass = float(getattr(config, "SLAB_BODIES", 0)) / max(state.n, 1)
+        self.super_bodies = 0
+        self.super_ws = None
+        if self.force_mode == "grouped":
+            self.set_super_bodies(int(getattr(config, "SUPER_BODIES", 0)))
         self.precision = _lib.PREC_F64 if getattr(config, "PRECISION", "f32") == "f64" else _lib.PREC_F32
         self.stage_events = None
+
+    def set_super_bodies(self, super_bodies):
+        """Two-level walk with super-buckets of at most `super_bodies` bodies
+        (0: single level).  Needs the grouped mode and the "ref_x" test."""
+        super_bodies = int(super_bodies)
+        if super_bodies == 0:
+            self.super_bodies, self.super_ws = 0, None
+            return
+        if self.force_mode != "grouped" or self.mac != _lib.MAC_REF_X:
+            raise ValueError("SUPER_BODIES needs FORCE_MODE 'grouped' and MAC 'ref_x'")
+        nbytes = int(_lib.load().cnb_two_level_workspace_bytes(self.state.n, super_bodies))
+        if nbytes < 0:
+            raise ValueError("SUPER_BODIES must be at least 32")
+        if self.super_ws is None or self.super_ws.numel() * 4 < nbytes:
+            self.super_ws = torch.empty((nbytes + 15) // 16, 4, dtype=torch.int32,
+                                        device=self.state.device)
+        self.super_bodies = super_bodies
 
     def _stream(self):
         return int(torch.cuda.current_stream(self.state.device).cuda_stream)
@@ -78,6 +102,14 @@ class SimulationEngine:
                     tm.node_table, tm.parent, tm.workspace, s.n, out=self.theta_per_group,
                     scale=self.controller_scale)
             tpg = self.theta_per_group
+            if self.super_ws is not None and tpg is None:
+                _lib.call("cnb_forces_two_level", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                          tm.node_table.data_ptr(), tm.ranges.data_ptr(), tm.parent.data_ptr(),
+                          tm.workspace.data_ptr(), self.super_ws.data_ptr(),
+                          self.super_ws.numel() * 4, self.super_bodies, s.force.data_ptr(), s.n,
+                          float(cfg.THETA), self.bodies_per_lane, self.block_warps, float(cfg.G),
+                          float(cfg.SOFTENING), float(cfg.BOX_SIZE), self.stats.data_ptr(), status, st)
+                return
             _lib.call("cnb_forces_grouped", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                       tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,
                       float(cfg.THETA), tpg.data_ptr() if tpg is not None else None, self.mac,

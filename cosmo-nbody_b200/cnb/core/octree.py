@@ -97,6 +97,14 @@ class OctreeManager:
                       self.bucket, self.workspace.data_ptr(), st)
         return self.root_idx
 
+    def validate(self):
+        """Check the topology of the current tree (raises CnbError if invalid)."""
+        from .._arrays import check_status
+        scratch = torch.empty(2 * max(self.n, 1), dtype=torch.int32, device=self.device)
+        _lib.call("cnb_validate_tree", self.child.data_ptr(), self.parent.data_ptr(), self.n,
+                  scratch.data_ptr(), status_buffer(self.device.index).data_ptr(), self._stream())
+        return check_status(self.device.index)
+
     def rebucket(self, max_size):
         """Rebuild the bucket table of the current tree with buckets of at most max_size bodies."""
         self.bucket = int(max_size)

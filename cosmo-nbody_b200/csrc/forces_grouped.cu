@@ -33,7 +33,7 @@
 
 namespace cnb {
 
-constexpr int kGStack = 1024;  // node stack entries per warp (deepest seen at 128^3: ~320)
+constexpr int kGStack = 512;   // node stack entries per warp (deepest seen at 128^3: ~320)
 constexpr int kGList = 64;     // interaction list entries per warp
 
 struct GroupedParams {
@@ -59,6 +59,14 @@ struct GroupedParams {
     unsigned long long *stats;  // [0] body-node interactions, [1] node tests,
                                 // [2] interactions needing the per-pair image (may be null)
     int32_t *status;
+    // two-level traversal: the bucket's super-bucket (k_super_lists) has already
+    // walked the top of the tree; null = walk from the root
+    const int32_t *super_of_body;  // super-bucket slot per body (-1: none)
+    const int4 *super_hdr;         // per super-bucket: (same-image, per-pair, near, complete)
+    const float4 *far_lists;       // per super-bucket: far_cap entries, same-image ones from the
+                                   // front, per-pair ones from the back
+    const int32_t *near_lists;     // per super-bucket: near_cap nodes left to each bucket
+    int far_cap, near_cap;
 };
 
 // Nearest-image offset of a coordinate difference d with |d| < 1.5:
@@ -97,8 +105,115 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
     }
 }
 
+// Two bodies per lane: the interaction list holds every entry twice over
+// (x, x, y, y | z, z, m, m), so a lane's two bodies form packed float2
+// operands and each FP32 instruction (FADD2 / FMUL2 / FFMA2, sm_100) serves
+// both.  The arithmetic, and its order, is the scalar loop's, so the forces
+// are bit-identical to it; only the minimum image is formed differently
+// (d - rint(d) through the 1.5 * 2^23 rounding constant, equal to image_of on
+// |d| < 1.5).
+template <bool WRAP>
+__device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, const float (&x)[2],
+                                                const float (&y)[2], const float (&z)[2],
+                                                float soft2, float (&ax)[2], float (&ay)[2],
+                                                float (&az)[2]) {
+    const float2 nx = make_float2(-x[0], -x[1]), ny = make_float2(-y[0], -y[1]),
+                 nz = make_float2(-z[0], -z[1]);
+    const float2 s2 = make_float2(soft2, soft2);
+    const float2 rc = make_float2(12582912.f, 12582912.f), nrc = make_float2(-12582912.f, -12582912.f);
+    const float2 m1 = make_float2(-1.f, -1.f);
+    float2 fx = make_float2(ax[0], ax[1]), fy = make_float2(ay[0], ay[1]),
+           fz = make_float2(az[0], az[1]);
+    // eight entries at a time: their loads, distances and inverse cubes are
+    // independent, then they are accumulated in list order
+    int j = 0;
+    for (; j + 8 <= cnt; j += 8) {
+        float2 dx[8], dy[8], dz[8], w[8], d2[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const float4 a = list[2 * (j + u)], b = list[2 * (j + u) + 1];
+            dx[u] = __fadd2_rn(make_float2(a.x, a.y), nx);
+            dy[u] = __fadd2_rn(make_float2(a.z, a.w), ny);
+            dz[u] = __fadd2_rn(make_float2(b.x, b.y), nz);
+            w[u] = make_float2(b.z, b.w);
+            if (WRAP) {
+                dx[u] = __ffma2_rn(__fadd2_rn(__fadd2_rn(dx[u], rc), nrc), m1, dx[u]);
+                dy[u] = __ffma2_rn(__fadd2_rn(__fadd2_rn(dy[u], rc), nrc), m1, dy[u]);
+                dz[u] = __ffma2_rn(__fadd2_rn(__fadd2_rn(dz[u], rc), nrc), m1, dz[u]);
+            }
+            d2[u] = __ffma2_rn(dx[u], dx[u], __ffma2_rn(dy[u], dy[u], __fmul2_rn(dz[u], dz[u])));
+        }
+        float2 f[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            const float2 q = __fadd2_rn(d2[u], s2);
+            float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
+            r0 = d2[u].x > 1e-7f ? r0 : 0.f;
+            r1 = d2[u].y > 1e-7f ? r1 : 0.f;
+            const float2 r = make_float2(r0, r1);
+            f[u] = __fmul2_rn(__fmul2_rn(__fmul2_rn(w[u], r), r), r);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            fx = __ffma2_rn(f[u], dx[u], fx);
+            fy = __ffma2_rn(f[u], dy[u], fy);
+            fz = __ffma2_rn(f[u], dz[u], fz);
+        }
+    }
+    for (; j < cnt; ++j) {
+        const float4 a = list[2 * j], b = list[2 * j + 1];
+        float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx);
+        float2 dy = __fadd2_rn(make_float2(a.z, a.w), ny);
+        float2 dz = __fadd2_rn(make_float2(b.x, b.y), nz);
+        if (WRAP) {
+            dx = __ffma2_rn(__fadd2_rn(__fadd2_rn(dx, rc), nrc), m1, dx);
+            dy = __ffma2_rn(__fadd2_rn(__fadd2_rn(dy, rc), nrc), m1, dy);
+            dz = __ffma2_rn(__fadd2_rn(__fadd2_rn(dz, rc), nrc), m1, dz);
+        }
+        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        const float2 q = __fadd2_rn(d2, s2);
+        float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
+        r0 = d2.x > 1e-7f ? r0 : 0.f;
+        r1 = d2.y > 1e-7f ? r1 : 0.f;
+        const float2 r = make_float2(r0, r1);
+        const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(b.z, b.w), r), r), r);
+        fx = __ffma2_rn(f, dx, fx);
+        fy = __ffma2_rn(f, dy, fy);
+        fz = __ffma2_rn(f, dz, fz);
+    }
+    ax[0] = fx.x; ax[1] = fx.y;
+    ay[0] = fy.x; ay[1] = fy.y;
+    az[0] = fz.x; az[1] = fz.y;
+}
+
+// float4 slots per list entry
+template <int BPL> __host__ __device__ constexpr int entry_width() { return BPL == 2 ? 2 : 1; }
+
+template <int BPL>
+__device__ __forceinline__ void put_entry(float4 *list, int idx, float4 e) {
+    if (BPL == 2) {
+        list[2 * idx] = make_float4(e.x, e.x, e.y, e.y);
+        list[2 * idx + 1] = make_float4(e.z, e.z, e.w, e.w);
+    } else {
+        list[idx] = e;
+    }
+}
+
+template <int BPL, bool WRAP>
+__device__ __forceinline__ void apply_entries(const float4 *list, int cnt, const float (&x)[BPL],
+                                              const float (&y)[BPL], const float (&z)[BPL],
+                                              float soft2, float (&ax)[BPL], float (&ay)[BPL],
+                                              float (&az)[BPL]) {
+    if constexpr (BPL == 2)
+        apply_list_pair<WRAP>(list, cnt, x, y, z, soft2, ax, ay, az);
+    else
+        apply_list<BPL, WRAP>(list, cnt, x, y, z, soft2, ax, ay, az);
+}
+
+template <int BPL>
 constexpr size_t grouped_smem(int warps) {
-    return (size_t)warps * (kGStack * sizeof(int32_t) + 2 * kGList * sizeof(float4));
+    return (size_t)warps * (kGStack * sizeof(int32_t) +
+                            2 * kGList * entry_width<BPL>() * sizeof(float4));
 }
 
 template <int BPL, int WARPS>
@@ -108,10 +223,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
     const uint32_t lt = (1u << lane) - 1u;
     // two interaction lists per warp: entries with one image for the whole
     // bucket, and entries needing the per-pair image
-    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * 2 * kGList;
-    float4 *wlist = list + kGList;
-    int32_t *stack = reinterpret_cast<int32_t *>(g_smem + WARPS * 2 * kGList * sizeof(float4)) +
-                     wib * kGStack;
+    constexpr int EW = entry_width<BPL>();
+    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * 2 * kGList * EW;
+    float4 *wlist = list + kGList * EW;
+    int32_t *stack =
+        reinterpret_cast<int32_t *>(g_smem + WARPS * 2 * kGList * EW * sizeof(float4)) +
+        wib * kGStack;
     unsigned long long n_tests = 0;
     int max_top = 0;
     bool overflow = false;
@@ -175,7 +292,37 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
         for (int b = 0; b < BPL; ++b) ax[b] = ay[b] = az[b] = 0.f;
         int top = 1, cnt = 0, wcnt = 0;
         unsigned long long n_entries = 0, n_wrap = 0;
-        if (lane == 0) stack[0] = root;
+        bool seeded = false;
+        if (P.super_of_body) {
+            const int sup = P.super_of_body[bk.x];
+            const int4 h = sup >= 0 ? P.super_hdr[sup] : make_int4(0, 0, 0, 0);
+            if (h.w) {
+                // the far field the super-bucket accepted holds for this bucket too
+                const float4 *far = P.far_lists + (int64_t)sup * P.far_cap;
+                for (int j0 = 0; j0 < h.x; j0 += 32) {
+                    const int c = min(32, h.x - j0);
+                    if (lane < c) put_entry<BPL>(list, lane, far[j0 + lane]);
+                    __syncwarp();
+                    apply_entries<BPL, false>(list, c, x, y, z, soft2, ax, ay, az);
+                    __syncwarp();
+                }
+                for (int j0 = 0; j0 < h.y; j0 += 32) {
+                    const int c = min(32, h.y - j0);
+                    if (lane < c) put_entry<BPL>(list, lane, far[P.far_cap - h.y + j0 + lane]);
+                    __syncwarp();
+                    apply_entries<BPL, true>(list, c, x, y, z, soft2, ax, ay, az);
+                    __syncwarp();
+                }
+                n_entries += h.x + h.y;
+                n_wrap += h.y;
+                // the near nodes it left are this bucket's starting stack
+                const int32_t *near = P.near_lists + (int64_t)sup * P.near_cap;
+                for (int j = lane; j < h.z; j += 32) stack[j] = near[j];
+                top = h.z;
+                seeded = true;
+            }
+        }
+        if (!seeded && lane == 0) stack[0] = root;
         __syncwarp();
         // a valid tree pushes every node at most once per bucket: more rounds
         // than nodes means a cyclic topology
@@ -198,9 +345,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             float4 E = make_float4(0.f, 0.f, 0.f, 0.f);
             int32_t c0 = -1, c1 = -1;
             if (node >= 0) {
+                // both halves of the record (one 32-byte sector) in flight together
                 const float4 A = __ldg(P.rec + 2 * node);
+                const float4 S = __ldg(P.rec + 2 * node + 1);
                 if (A.w > 0.f) {
-                    const float4 S = __ldg(P.rec + 2 * node + 1);
                     c0 = __float_as_int(S.z);
                     c1 = __float_as_int(S.w);
                     float dx = A.x - gcx, dy = A.y - gcy, dz = A.z - gcz;
@@ -247,9 +395,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             const uint32_t nm = am & ~wm;
             if (accept) {
                 if (to_w)
-                    wlist[wcnt + __popc(wm & lt)] = make_float4(E.x, E.y, E.z, -E.w);
+                    put_entry<BPL>(wlist, wcnt + __popc(wm & lt), make_float4(E.x, E.y, E.z, -E.w));
                 else
-                    list[cnt + __popc(nm & lt)] = E;
+                    put_entry<BPL>(list, cnt + __popc(nm & lt), E);
             }
             cnt += __popc(nm);
             wcnt += __popc(wm);
@@ -267,25 +415,29 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             }
             __syncwarp();
             if (cnt >= 32) {
-                apply_list<BPL, false>(list, 32, x, y, z, soft2, ax, ay, az);
+                apply_entries<BPL, false>(list, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 __syncwarp();
-                if (lane < cnt - 32) list[lane] = list[32 + lane];
+#pragma unroll
+                for (int w = 0; w < EW; ++w)
+                    if (lane < cnt - 32) list[EW * lane + w] = list[EW * (32 + lane) + w];
                 cnt -= 32;
                 __syncwarp();
             }
             if (wcnt >= 32) {
-                apply_list<BPL, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
+                apply_entries<BPL, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 n_wrap += 32;
                 __syncwarp();
-                if (lane < wcnt - 32) wlist[lane] = wlist[32 + lane];
+#pragma unroll
+                for (int w = 0; w < EW; ++w)
+                    if (lane < wcnt - 32) wlist[EW * lane + w] = wlist[EW * (32 + lane) + w];
                 wcnt -= 32;
                 __syncwarp();
             }
         }
-        apply_list<BPL, false>(list, cnt, x, y, z, soft2, ax, ay, az);
-        apply_list<BPL, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
+        apply_entries<BPL, false>(list, cnt, x, y, z, soft2, ax, ay, az);
+        apply_entries<BPL, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
         n_entries += cnt + wcnt;
         n_wrap += wcnt;
         __syncwarp();
@@ -312,6 +464,155 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
         if (lane == 0) atomicAdd(P.stats + 1, n_tests);
     }
     if (lane == 0) atomicMax(P.ws + 2, max_top);
+}
+
+// ---------------------------------------------------------------- two-level
+// One warp per super-bucket S (a maximal subtree of at most super_bodies
+// bodies) walks the top of the tree once, for every bucket inside S, with the
+// reference opening test.  With dmin / dmax the smallest / largest distance
+// any point of S's box can have to the node's CoM (per axis, periodic):
+//   s^2 <  theta^2 dmin^2  every bucket of S accepts the node  -> far list
+//   s^2 >= theta^2 dmax^2  every bucket of S opens it           -> push children
+//   otherwise              the bucket decides                   -> near list
+// (leaves always go to the far list, as a bucket accepts every leaf it
+// reaches).  A bucket b inside S has dmin(S) <= dmin(b) <= dmax(S), so the
+// nodes a bucket accepts from S's far list plus its own walk from S's near
+// nodes are exactly the nodes it accepts walking from the root.  A far entry
+// keeps one image for all of S when S lies within half a box of it on every
+// axis (then it is the minimum image for every body of S), otherwise it is
+// stored for the per-pair minimum image.  A super-bucket whose lists or stack
+// do not fit is marked incomplete; its buckets then walk from the root.
+struct SuperParams {
+    const float4 *rec, *aabb;
+    const int32_t *sws;     // [0] super-bucket count, [1] work counter, [2] incomplete count
+    const int4 *supers;     // (first body, count, subtree node, 0)
+    int4 *hdr;              // (same-image, per-pair, near, complete) per listed super-bucket
+    int32_t *super_of_body; // listed super-bucket of each body, -1 if none
+    float4 *far;            // far_cap per super-bucket: same-image from the front, per-pair from the back
+    int32_t *near;          // near_cap per super-bucket
+    int far_cap, near_cap, max_listed;
+    float th2, box, half_box;
+    int64_t m_nodes;
+    int32_t root;
+    unsigned long long *stats;
+    int32_t *status;
+};
+
+constexpr int kSWarps = 8;
+
+__global__ void __launch_bounds__(kSWarps * 32) k_super_lists(SuperParams P) {
+    __shared__ int32_t stacks[kSWarps][kGStack];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint32_t lt = (1u << lane) - 1u;
+    int32_t *stack = stacks[wib];
+    const int n_sup = P.sws[0];
+    unsigned long long n_tests = 0;
+    for (;;) {
+        int s = 0;
+        if (lane == 0) s = atomicAdd(const_cast<int32_t *>(P.sws) + 1, 1);
+        s = __shfl_sync(0xffffffffu, s, 0);
+        if (s >= n_sup) break;
+        const int4 sb = P.supers[s];
+        const bool listed = s < P.max_listed;
+        for (int k = lane; k < sb.y; k += 32) P.super_of_body[sb.x + k] = listed ? s : -1;
+        if (!listed) continue;
+        const float4 blo = __ldg(P.aabb + 2 * sb.z), bhi = __ldg(P.aabb + 2 * sb.z + 1);
+        const float gx = 0.5f * (blo.x + bhi.x), gy = 0.5f * (blo.y + bhi.y), gz = 0.5f * (blo.z + bhi.z);
+        const float hx = 0.5f * (bhi.x - blo.x), hy = 0.5f * (bhi.y - blo.y), hz = 0.5f * (bhi.z - blo.z);
+        const float wlx = 0.5f - hx - 1e-6f, wly = 0.5f - hy - 1e-6f, wlz = 0.5f - hz - 1e-6f;
+        float4 *far = P.far + (int64_t)s * P.far_cap;
+        int32_t *near = P.near + (int64_t)s * P.near_cap;
+        int top = 1, n_same = 0, n_wrap = 0, n_near = 0;
+        bool ok = true;
+        if (lane == 0) stack[0] = P.root;
+        __syncwarp();
+        int64_t rounds = 0;
+        while (top > 0) {
+            if (++rounds > P.m_nodes) {
+                if (lane == 0) set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
+                ok = false;
+                break;
+            }
+            const int k = top < 32 ? top : 32;
+            top -= k;
+            int32_t node = -1;
+            if (lane < k) node = stack[top + lane];
+            __syncwarp();
+            if (node >= P.m_nodes) {
+                set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
+                node = -1;
+            }
+            // 1: far, one image   2: far, per-pair image   3: open   4: near
+            int cls = 0;
+            float4 E = make_float4(0.f, 0.f, 0.f, 0.f);
+            int32_t c0 = -1, c1 = -1;
+            if (node >= 0) {
+                const float4 A = __ldg(P.rec + 2 * node);
+                const float4 S = __ldg(P.rec + 2 * node + 1);
+                if (A.w > 0.f) {
+                    c0 = __float_as_int(S.z);
+                    c1 = __float_as_int(S.w);
+                    float dx = A.x - gx, dy = A.y - gy, dz = A.z - gz;
+                    const float sx_ = image_of(dx), sy_ = image_of(dy), sz_ = image_of(dz);
+                    dx -= sx_;
+                    dy -= sy_;
+                    dz -= sz_;
+                    const float adx = fabsf(dx), ady = fabsf(dy), adz = fabsf(dz);
+                    const int far_cls = (adx < wlx && ady < wly && adz < wlz) ? 1 : 2;
+                    if (c0 == -1) {
+                        cls = far_cls;
+                    } else {
+                        const float s = S.x > P.half_box ? P.box : S.x;
+                        const float tx = fmaxf(adx - hx, 0.f), ty = fmaxf(ady - hy, 0.f),
+                                    tz = fmaxf(adz - hz, 0.f);
+                        if (s * s < P.th2 * (tx * tx + ty * ty + tz * tz)) {
+                            cls = far_cls;
+                        } else {
+                            const float ux = fminf(adx + hx, P.half_box),
+                                        uy = fminf(ady + hy, P.half_box),
+                                        uz = fminf(adz + hz, P.half_box);
+                            cls = (s * s >= P.th2 * (ux * ux + uy * uy + uz * uz)) ? 3 : 4;
+                        }
+                    }
+                    E = make_float4(A.x - sx_, A.y - sy_, A.z - sz_, A.w);
+                }
+            }
+            n_tests += (node >= 0);
+            const uint32_t m1 = __ballot_sync(0xffffffffu, cls == 1);
+            const uint32_t m2 = __ballot_sync(0xffffffffu, cls == 2);
+            const uint32_t m3 = __ballot_sync(0xffffffffu, cls == 3);
+            const uint32_t m4 = __ballot_sync(0xffffffffu, cls == 4);
+            const int c_same = __popc(m1), c_wrap = __popc(m2), c_open = __popc(m3),
+                      c_near = __popc(m4);
+            if (n_same + c_same + n_wrap + c_wrap > P.far_cap || n_near + c_near > P.near_cap ||
+                top + 2 * c_open > kGStack) {
+                ok = false;
+                break;
+            }
+            if (cls == 1) far[n_same + __popc(m1 & lt)] = E;
+            if (cls == 2) far[P.far_cap - 1 - (n_wrap + __popc(m2 & lt))] = E;
+            if (cls == 4) near[n_near + __popc(m4 & lt)] = node;
+            if (cls == 3) {
+                const int pos = top + 2 * __popc(m3 & lt);
+                stack[pos] = c1;
+                stack[pos + 1] = c0;
+            }
+            n_same += c_same;
+            n_wrap += c_wrap;
+            n_near += c_near;
+            top += 2 * c_open;
+            __syncwarp();
+        }
+        __syncwarp();
+        if (lane == 0) {
+            P.hdr[s] = make_int4(n_same, n_wrap, n_near, ok ? 1 : 0);
+            if (!ok) atomicAdd(const_cast<int32_t *>(P.sws) + 2, 1);
+        }
+    }
+    if (P.stats) {
+        for (int o = 16; o > 0; o >>= 1) n_tests += __shfl_xor_sync(0xffffffffu, n_tests, o);
+        if (lane == 0) atomicAdd(P.stats + 1, n_tests);
+    }
 }
 
 // Traversal node table from the reference-layout tree: 32-byte records
@@ -359,7 +660,7 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
 
 template <int BPL, int WARPS>
 static int launch_shape(GroupedParams &P, cudaStream_t st) {
-    const size_t smem = grouped_smem(WARPS);
+    const size_t smem = grouped_smem<BPL>(WARPS);
     CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -433,6 +734,97 @@ extern "C" int cnb_forces_grouped(const float *px, const float *py, const float 
     P.box = (float)box;
     P.slab_mass = (float)slab_mass;
     return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
+}
+
+// Two-level workspace (bytes from offset 0, each part 16-byte aligned):
+//   16 B header | supers int4[n] | hdr int4[L] | super_of_body int32[n] |
+//   near int32[L * near_cap] | far float4[L * far_cap]
+// with L the number of super-bucket list slots the given size holds.
+static constexpr int kFarCap = 2048, kNearCap = 256;
+
+static int64_t align16(int64_t b) { return (b + 15) & ~(int64_t)15; }
+
+static int64_t two_level_fixed_bytes(int64_t n) {
+    return 16 + 16 * n + align16(4 * n);
+}
+
+static int64_t two_level_slot_bytes() {
+    return 16 + 4LL * kNearCap + 16LL * kFarCap;
+}
+
+extern "C" int64_t cnb_two_level_workspace_bytes(int64_t n, int super_bodies) {
+    if (n < 0 || super_bodies < 32) return -1;
+    // super-buckets average well over a quarter of the limit; the rest walk from the root
+    int64_t slots = 4 * n / super_bodies + 64;
+    if (slots > n) slots = n > 0 ? n : 1;
+    return two_level_fixed_bytes(n) + slots * two_level_slot_bytes();
+}
+
+extern "C" int cnb_forces_two_level(const float *px, const float *py, const float *pz,
+                                    const float *node_table, const int32_t *ranges,
+                                    const int32_t *parents, int32_t *workspace,
+                                    void *super_ws, int64_t super_ws_bytes, int super_bodies,
+                                    float *force, int64_t n, double theta, int bodies_per_lane,
+                                    int block_warps, double G, double soft, double box,
+                                    unsigned long long *stats, int32_t *status, void *stream) {
+    GroupedParams P;
+    CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, nullptr, CNB_MAC_REF_X,
+                           bodies_per_lane, block_warps, G, stats, status));
+    if (n == 0) return CNB_OK;
+    if (!super_ws || (reinterpret_cast<uintptr_t>(super_ws) & 15) || super_bodies < 32 ||
+        (n > 1 && (!ranges || !parents)))
+        return CNB_E_INVALID_ARG;
+    const int64_t fixed = two_level_fixed_bytes(n);
+    if (super_ws_bytes < fixed + two_level_slot_bytes()) return CNB_E_INVALID_ARG;
+    int64_t slots = (super_ws_bytes - fixed) / two_level_slot_bytes();
+    if (slots > n) slots = n;
+    if (slots > INT32_MAX) slots = INT32_MAX;
+    cudaStream_t st = as_stream(stream);
+    P.theta = (float)theta;
+    P.soft2 = (float)(soft * soft);
+    P.box = (float)box;
+
+    unsigned char *base = static_cast<unsigned char *>(super_ws);
+    int32_t *sws = reinterpret_cast<int32_t *>(base);
+    const int4 *supers = reinterpret_cast<const int4 *>(base + 16);
+    int4 *hdr = reinterpret_cast<int4 *>(base + 16 + 16 * n);
+    int32_t *super_of_body = reinterpret_cast<int32_t *>(base + 16 + 16 * n + 16 * slots);
+    int32_t *near = reinterpret_cast<int32_t *>(base + 16 + 16 * n + 16 * slots + align16(4 * n));
+    float4 *far = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(near) +
+                                             4LL * kNearCap * slots);
+    CNB_TRY(cnb_make_buckets(ranges, parents, n, super_bodies, sws, stream));
+
+    SuperParams S{};
+    S.rec = P.rec;
+    S.aabb = P.aabb;
+    S.sws = sws;
+    S.supers = supers;
+    S.hdr = hdr;
+    S.super_of_body = super_of_body;
+    S.far = far;
+    S.near = near;
+    S.far_cap = kFarCap;
+    S.near_cap = kNearCap;
+    S.max_listed = (int)slots;
+    S.th2 = (float)(theta * theta);
+    S.box = P.box;
+    S.half_box = 0.5f * P.box;
+    S.m_nodes = P.m_nodes;
+    S.root = P.root;
+    S.stats = stats;
+    S.status = status;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_super_lists, kSWarps * 32, 0);
+    k_super_lists<<<kSMs * (per_sm > 0 ? per_sm : 1), kSWarps * 32, 0, st>>>(S);
+    CNB_TRY(launch_status());
+
+    P.super_of_body = super_of_body;
+    P.super_hdr = hdr;
+    P.far_lists = far;
+    P.near_lists = near;
+    P.far_cap = kFarCap;
+    P.near_cap = kNearCap;
+    return launch_grouped(P, bodies_per_lane, block_warps, st);
 }
 
 extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,

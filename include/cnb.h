@@ -108,6 +108,13 @@ int cnb_reset_tree_buffers(int32_t *child, int32_t *parent, int32_t *counters,
 int cnb_build_tree(const uint64_t *codes, int32_t *children, int32_t *parents, int64_t n,
                    void *stream);
 
+/* Topology check (no reference counterpart): every node but one root is the
+ * child of exactly one internal node and parents[] agrees with children[];
+ * otherwise CNB_FLAG_BAD_TOPOLOGY is set in status.  scratch: device int32
+ * [2N] (overwritten). */
+int cnb_validate_tree(const int32_t *children, const int32_t *parents, int64_t n,
+                      int32_t *scratch, int32_t *status, void *stream);
+
 /* src/kernels/tree_kernels.py:131-191 compute_multipoles(pos_x, pos_y, pos_z, mass,
  * children, parents, n_mass, n_com, n_min, n_max, counts).  n = bodies. */
 int cnb_compute_multipoles(const float *px, const float *py, const float *pz,
@@ -230,6 +237,24 @@ int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                        double theta, const float *theta_per_bucket, int mac, int bodies_per_lane,
                        int block_warps, double G, double soft, double box, double slab_mass,
                        unsigned long long *stats, int32_t *status, void *stream);
+
+/* Two-level form of cnb_forces_grouped (no reference counterpart; same
+ * results as CNB_MAC_REF_X up to float32 summation order).  The tree is cut
+ * into super-buckets (maximal subtrees of at most super_bodies bodies, >= 32);
+ * one warp per super-bucket walks the top of the tree once and keeps the
+ * nodes every bucket inside it accepts (applied by each bucket from that
+ * list) and the nodes only a bucket can decide (each bucket's walk starts
+ * there).  ranges / parents: cnb_build_tree_ranges; workspace: the bucket
+ * table of cnb_make_buckets; super_ws: device scratch of super_ws_bytes
+ * (16-byte aligned), cnb_two_level_workspace_bytes recommends a size; a
+ * super-bucket whose lists do not fit there walks from the root. */
+int64_t cnb_two_level_workspace_bytes(int64_t n, int super_bodies);
+int cnb_forces_two_level(const float *px, const float *py, const float *pz,
+                         const float *node_table, const int32_t *ranges, const int32_t *parents,
+                         int32_t *workspace, void *super_ws, int64_t super_ws_bytes,
+                         int super_bodies, float *force, int64_t n, double theta,
+                         int bodies_per_lane, int block_warps, double G, double soft, double box,
+                         unsigned long long *stats, int32_t *status, void *stream);
 
 /* src/utils/visualizer.py:115-171 colorize_frame (+ the 8-bit packing of
  * src/core/engine.py:139): grid [height, width] float32 -> rgb float32
