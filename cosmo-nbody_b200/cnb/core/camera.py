@@ -56,18 +56,20 @@ class Camera:
                   self.height, st)
         return self.grid_d
 
-    def colorize(self, out_u8=None):
+    def colorize(self, out_u8=None, out=None):
         """visualizer.py:115-171 on the current grid in two fused kernels;
-        returns the float32 [H, W, 3] frame (and fills `out_u8`, uint8
-        [H, W, 3], with the engine.py:139 packing when given)."""
+        returns the float32 [H, W, 3] frame (written to `out` when given, else
+        to the camera's own buffer) and fills `out_u8`, uint8 [H, W, 3], with
+        the engine.py:139 packing when given."""
         if not hasattr(self, "frame_d"):
             self.frame_d = torch.empty((self.height, self.width, 3), dtype=torch.float32, device=self.device)
             self._cmax = torch.zeros(1, dtype=torch.int32, device=self.device)
+        frame = self.frame_d if out is None else out
         st = int(torch.cuda.current_stream(self.device).cuda_stream)
         _lib.call("cnb_colorize", self.grid_d.data_ptr(), self.width, self.height,
-                  self.frame_d.data_ptr(), out_u8.data_ptr() if out_u8 is not None else None,
+                  frame.data_ptr(), out_u8.data_ptr() if out_u8 is not None else None,
                   self._cmax.data_ptr(), st)
-        return self.frame_d
+        return frame
 
     def capture(self, step, px_d, py_d, pz_d):
         """camera.py:29-48: splat and colourise; returns the [H, W, 3] frame."""

@@ -150,9 +150,10 @@ class SimulationEngine:
         self.a += self.da
 
     # ------------------------------------------------------------ CUDA graph
-    def _step_device(self, mvp=None):
+    def _step_device(self, mvp=None, frame=None):
         """One step with no host scalars (a, H, dt live on the device), so it
-        can be captured; `mvp` (device [4,4]) also splats the new positions."""
+        can be captured; `mvp` (device [4,4]) also splats the new positions
+        and `frame` (device [H, W, 3]) receives their colourised grid."""
         self.forces_only()
         a = self.a_dev
         cfg = self.config
@@ -166,25 +167,42 @@ class SimulationEngine:
         self.a_dev += self.da
         if mvp is not None and self.camera is not None:
             self.camera.splat_device(mvp, *s.pos)
+            if frame is not None:
+                self.camera.colorize(out=frame)
 
-    def capture(self, splat=True):
+    def capture(self, splat=True, colorize=False, step0=0):
         """Capture two consecutive steps (and their splats) in one CUDA graph.
         The step alternates between two array sets, so after every replay the
-        arrays are back where they were captured.  Use replay() afterwards."""
-        self.a_dev = torch.tensor([self.a], dtype=torch.float64, device=self.state.device)
-        self.aHdt = torch.zeros((1, 3), dtype=torch.float64, device=self.state.device)
-        self.mvp_slots = torch.zeros((2, 4, 4), dtype=torch.float32, device=self.state.device)
+        arrays are back where they were captured.  The two steps that run
+        eagerly first (steps step0, step0 + 1 of the camera orbit) warm up
+        the capture.  With `colorize`, each step's frame lands in
+        `frame_slots[k]`.  Use replay() afterwards."""
+        dev = self.state.device
+        self.a_dev = torch.tensor([self.a], dtype=torch.float64, device=dev)
+        self.aHdt = torch.zeros((1, 3), dtype=torch.float64, device=dev)
+        self.mvp_slots = torch.zeros((2, 4, 4), dtype=torch.float32, device=dev)
         self._graph_splat = bool(splat and self.camera is not None)
-        self._step_device(self.mvp_slots[0] if self._graph_splat else None)   # warm-up, eager
-        self._step_device(self.mvp_slots[1] if self._graph_splat else None)
+        self.frame_slots = None
+        if self._graph_splat:
+            for k in range(2):
+                self.mvp_slots[k].copy_(self.camera.mvp_host(step0 + k))
+            if colorize:
+                self.frame_slots = torch.empty((2, self.camera.height, self.camera.width, 3),
+                                               dtype=torch.float32, device=dev)
+
+        def two_steps():
+            for k in range(2):
+                self._step_device(self.mvp_slots[k] if self._graph_splat else None,
+                                  self.frame_slots[k] if self.frame_slots is not None else None)
+
+        two_steps()                      # warm-up, eager
         self.a += 2 * self.da
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            for k in range(2):
-                self._step_device(self.mvp_slots[k] if self._graph_splat else None)
+            two_steps()
         self._graph = g
-        self._graph_step = 2
+        self._graph_step = step0 + 2
         return g
 
     def replay(self):
@@ -213,13 +231,41 @@ class SimulationEngine:
             self.stage_events = []
         return out
 
-    def run(self, n_steps=None, frames=False):
+    def run(self, n_steps=None, frames=False, graph=None):
         """engine.py:125-139 without the host video buffer: steps, captures a
-        frame per step, returns the last frame (or all frames if `frames`)."""
+        frame per step, returns the last frame (or all frames if `frames`).
+        With `graph` (default: grouped mode and at least 4 steps) the steps
+        run as replays of one captured two-step graph, frames included, with
+        no host synchronisation between them; an odd last step runs eagerly."""
         n_steps = self.config.N_STEPS if n_steps is None else n_steps
+        if graph is None:
+            graph = self.force_mode == "grouped" and n_steps >= 4
         out = []
         frame = None
-        for i in range(n_steps):
+        i = 0
+        if graph and n_steps >= 2:
+            self.capture(splat=True, colorize=True, step0=0)     # runs steps 0 and 1
+            i = 2
+            while True:
+                if self.frame_slots is not None:
+                    frame = self.frame_slots[1]
+                    if frames:
+                        out.extend(f.clone() for f in self.frame_slots)
+                if i + 2 > n_steps:
+                    break
+                self.replay()
+                i += 2
+            self._graph = None
+            if i < n_steps:
+                # the device scalars carry a, so the odd last step takes them too
+                self._step_device()
+                self.a += self.da
+                i += 1
+                if self.camera is not None:
+                    frame = self.camera.capture(i - 1, *self.state.pos)
+                    if frames:
+                        out.append(frame.clone())
+        for i in range(i, n_steps):
             self.step()
             if self.camera is not None:
                 frame = self.camera.capture(i, *self.state.pos)

@@ -279,3 +279,54 @@ def test_device_step_matches_host_step():
         b_eng._step_device()
     for a, b in zip(a_eng.state.pos + a_eng.state.vel, b_eng.state.pos + b_eng.state.vel):
         np.testing.assert_allclose(host(a), host(b), rtol=1e-6, atol=1e-7)
+
+
+@pytest.mark.parametrize("n_steps", [5, 4])
+def test_run_replays_graph_with_frames(n_steps):
+    """run() as graph replays (frames included) equals the same device-scalar
+    steps run one by one, frame by frame."""
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = config(16, KEY_MODE="morton63", FORCE_MODE="grouped", RES_W=96, RES_H=54)
+    pos, vel = zeldovich_arrays(16, 7)
+    graphed = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel))
+    frames_g = graphed.run(n_steps=n_steps, frames=True, graph=True)
+    eager = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel))
+    eager.a_dev = torch.tensor([eager.a], dtype=torch.float64, device="cuda")
+    eager.aHdt = torch.zeros((1, 3), dtype=torch.float64, device="cuda")
+    mvp = torch.zeros((4, 4), device="cuda")
+    frames_e = []
+    for k in range(n_steps):
+        mvp.copy_(eager.camera.mvp_host(k))
+        eager._step_device(mvp)
+        eager.a += eager.da
+        frames_e.append(eager.camera.colorize().clone())
+    torch.cuda.synchronize()
+    assert len(frames_g) == n_steps
+    for a, b in zip(eager.state.pos + eager.state.vel, graphed.state.pos + graphed.state.vel):
+        np.testing.assert_array_equal(host(a), host(b))
+    for fe, fg in zip(frames_e, frames_g):
+        np.testing.assert_allclose(host(fe), host(fg), rtol=1e-4, atol=1e-6)
+    assert abs(graphed.a - eager.a) < 1e-12
+    # and close to the host-scalar step of the reference's loop
+    plain = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel))
+    plain.run(n_steps=n_steps, graph=False)
+    for a, b in zip(plain.state.pos + plain.state.vel, graphed.state.pos + graphed.state.vel):
+        np.testing.assert_allclose(host(a), host(b), rtol=1e-5, atol=1e-6)
+
+
+def test_device_initial_conditions_match_host_generator():
+    from cnb.utils import config as cfgmod
+    from cnb.utils.cosmology import generate_zeldovich_ics, zeldovich_arrays
+    for n in (32, 64):
+        cfg = cfgmod.make(N_GRID=n, SEED=3)
+        pos_d, vel_d = generate_zeldovich_ics(cfg, device="cuda")
+        pos_h, vel_h = zeldovich_arrays(n, 3, cfg.A_START, cfg.H0, cfg.OMEGA_M, cfg.OMEGA_L)
+        for d, h in zip(pos_d + vel_d, pos_h + vel_h):
+            assert d.is_cuda and d.dtype == torch.float32
+            d = host(d)
+            # cuFFT and numpy's FFT differ in the last float64 bits: float32 values agree to 1 ulp
+            ulp = np.spacing(np.abs(h)).astype(np.float64)
+            assert np.all(np.abs(d.astype(np.float64) - h) <= ulp)
+            assert np.mean(d == h) > 0.99
