@@ -10,7 +10,7 @@ import numpy as np
 import torch
 
 from ._lib import CnbError, FLAG_BAD_TOPOLOGY, FLAG_LIST_OVERFLOW, FLAG_NONFINITE, \
-    FLAG_STACK_OVERFLOW
+    FLAG_STACK_OVERFLOW, FLAG_WAIT_LIMIT
 
 _TYPESTR = {
     np.dtype(np.float32): "<f4",
@@ -92,6 +92,7 @@ FLAG_NAMES = {
     FLAG_BAD_TOPOLOGY: "invalid tree topology",
     FLAG_NONFINITE: "non-finite acceleration",
     FLAG_LIST_OVERFLOW: "grouped traversal work queue exhausted",
+    FLAG_WAIT_LIMIT: "a bounded wait between blocks gave up (sort result invalid)",
 }
 
 
@@ -108,7 +109,8 @@ def read_status(device=None, clear=True):
     return val
 
 
-def check_status(device=None, fatal=FLAG_BAD_TOPOLOGY | FLAG_NONFINITE | FLAG_LIST_OVERFLOW):
+def check_status(device=None,
+                 fatal=FLAG_BAD_TOPOLOGY | FLAG_NONFINITE | FLAG_LIST_OVERFLOW | FLAG_WAIT_LIMIT):
     """Raise CnbError if a fatal flag was raised since the last check."""
     val = read_status(device)
     if val & fatal:

@@ -23,6 +23,7 @@ FLAG_STACK_OVERFLOW = 1
 FLAG_BAD_TOPOLOGY = 2
 FLAG_NONFINITE = 4
 FLAG_LIST_OVERFLOW = 8
+FLAG_WAIT_LIMIT = 16
 
 KEY_COMPAT30 = 0
 KEY_MORTON63 = 1
@@ -52,6 +53,7 @@ SIGNATURES = {
     "cnb_ctx_destroy": (_int, [_p]),
     "cnb_sort_pairs": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
     "cnb_sort_pairs_noalloc": (_int, [_p, _p, _p, _p, _i64, _int, _p]),
+    "cnb_ctx_take_flags": (_int, [_p, _p, _p]),
     "cnb_gather_f32": (_int, [_p, _int, _p, _p, _i64, _p]),
     "cnb_reset_tree_buffers": (_int, [_p, _p, _p, _p, _i64, _p]),
     "cnb_build_tree": (_int, [_p, _p, _p, _i64, _p]),

@@ -22,6 +22,7 @@ import numpy as np
 import torch
 
 from .. import _lib
+from .._arrays import status_buffer
 from ..kernels.morton import KEY_BITS, KEY_MODES
 
 
@@ -41,9 +42,14 @@ class SortContext:
         _lib.call("cnb_ctx_create", int(n_max), C.byref(self.ptr))
         self.n_max = int(n_max)
 
-    def sort_pairs(self, keys_in, keys_out, idx_in, perm_out, n, key_bits, stream):
+    def sort_pairs(self, keys_in, keys_out, idx_in, perm_out, n, key_bits, stream, status=None):
+        """Stable (key, index) sort; the sort's device flags are ORed into
+        `status` (the shared device status word when None)."""
         _lib.call("cnb_sort_pairs", self.ptr, keys_in, keys_out, idx_in, perm_out, int(n),
                   int(key_bits), stream)
+        if status is None:
+            status = status_buffer().data_ptr()
+        _lib.call("cnb_ctx_take_flags", self.ptr, status, stream)
 
     def close(self):
         if self.ptr:

@@ -10,6 +10,11 @@ struct cnb_ctx {
     uint64_t *keys_tmp[2] = {nullptr, nullptr};
     uint32_t *vals_tmp[2] = {nullptr, nullptr};
     uint32_t *tile_hist = nullptr;  // [256 * (tiles_max + 1)]: digit-major counts, digit totals
+                                    // (reduce-then-scan sort of cnb_sort_pairs_noalloc)
+    // one-sweep sort: [8 x 256] digit counts of every pass, [8] tile counters,
+    // then the look-back words of every pass, [8 x tiles x 256] (2048-key tiles)
+    uint32_t *sweep = nullptr;
+    int32_t *flags = nullptr;       // CNB_FLAG_* raised by the sort, taken by cnb_ctx_take_flags
     // grouped traversal scratch (grown on demand by cnb_forces_grouped)
     void *group_scratch = nullptr;
     size_t group_scratch_bytes = 0;
@@ -19,4 +24,11 @@ namespace cnb {
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
+constexpr int kSweepPasses = 8;                        // 8-bit digits of keys up to 64 bits
+constexpr int64_t kSweepMetaWords = kSweepPasses * 256 + 64;  // counts, tile counters, padding
+// bytes of the one-sweep scratch for up to n_max keys (tiles of 2048 keys)
+inline int64_t sweep_bytes(int64_t n_max) {
+    const int64_t tiles = (n_max + 2047) / 2048;
+    return kSweepMetaWords * 4 + (int64_t)kSweepPasses * tiles * 256 * 8;
+}
 }  // namespace cnb

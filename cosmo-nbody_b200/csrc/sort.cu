@@ -1,15 +1,22 @@
 // sort.cu -- stable LSD radix sort of (Morton key, index) pairs and the
 // permutation gathers (src/core/state.py:20-40: cp.argsort + 8 gathers).
 //
-// One pass per 8-bit digit, reduce-then-scan (no inter-block waiting):
-//   k_digit_count   per-tile digit counts (shared-memory histograms)
-//   k_scan_rows     exclusive scan of each digit's tile counts (one block
-//                   per digit) and the digit totals
-//   k_scatter       stable in-tile ranks (warp __match_any_sync + per-warp
-//                   digit counters), the tile reordered by digit in shared
-//                   memory, then coalesced runs written to global positions
-// A 4096-key tile per 256-thread block keeps one pass at 8 B read for the
-// count, 12 B read + 12 B written for the scatter, per key.
+// cnb_sort_pairs, one sweep per 8-bit digit:
+//   k_digit_hist_all  the counts of every digit of every pass, one read of
+//                     the keys (runs of equal digits summed in registers)
+//   k_onesweep        per 2048-key tile (tiles handed out in order by an
+//                     atomic counter): stable in-tile ranks (warp
+//                     __match_any_sync + per-warp digit counters), the tile's
+//                     digit counts published at once, the counts of earlier
+//                     tiles gathered by looking back at what they published
+//                     (bounded waits on tiles that already started), the tile
+//                     reordered by digit in shared memory and written out in
+//                     coalesced runs
+// One pass reads 12 B and writes 12 B per key.  Tiles are 2048 keys.
+//
+// cnb_sort_pairs_noalloc keeps the reduce-then-scan form, which never waits
+// on another block: per pass k_digit_count (per-tile counts), k_scan_rows
+// (one block per digit) and k_scatter.
 #include <new>
 
 #include "ctx.cuh"
@@ -200,6 +207,245 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t *__rest
     }
 }
 
+// ---------------------------------------------------------------- one sweep
+// Counts of every digit of the first `passes` passes.  Each thread sums
+// runs of equal digits over kSortItems consecutive keys before touching the
+// shared histograms (sorted or nearly sorted input repeats its high digits).
+__global__ void __launch_bounds__(kSortThreads) k_digit_hist_all(const uint64_t *__restrict__ keys,
+                                                                 int64_t n, int passes,
+                                                                 uint32_t *__restrict__ hist) {
+    __shared__ uint32_t sh[kSweepPasses][256];
+    for (int i = threadIdx.x; i < kSweepPasses * 256; i += kSortThreads) (&sh[0][0])[i] = 0;
+    __syncthreads();
+    for (int64_t base = ((int64_t)blockIdx.x * kSortThreads + threadIdx.x) * kSortItems; base < n;
+         base += (int64_t)gridDim.x * kSortThreads * kSortItems) {
+        const int cnt = (int)min((int64_t)kSortItems, n - base);
+        uint64_t kk[kSortItems];
+#pragma unroll
+        for (int k = 0; k < kSortItems; ++k) kk[k] = (k < cnt) ? __ldg(keys + base + k) : 0;
+        for (int p = 0; p < passes; ++p) {
+            const int shift = 8 * p;
+            uint32_t cur = (uint32_t)(kk[0] >> shift) & 255u, run = 1;
+#pragma unroll
+            for (int k = 1; k < kSortItems; ++k) {
+                if (k < cnt) {
+                    const uint32_t d = (uint32_t)(kk[k] >> shift) & 255u;
+                    if (d == cur) {
+                        ++run;
+                    } else {
+                        atomicAdd(&sh[p][cur], run);
+                        cur = d;
+                        run = 1;
+                    }
+                }
+            }
+            atomicAdd(&sh[p][cur], run);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < passes * 256; i += kSortThreads) {
+        const uint32_t v = (&sh[0][0])[i];
+        if (v) atomicAdd(hist + i, v);
+    }
+}
+
+// Look-back words: the tile's count of one digit in the low 32 bits, the
+// state above (0: not yet published, 1: this tile's count only, 2: the
+// count of this and every earlier tile).
+constexpr uint64_t kLbCount = 1ull << 32, kLbPrefix = 2ull << 32;
+// the one-sweep tile and how many earlier tiles one look-back step reads
+constexpr int kSweepItems = 16;
+constexpr int kLookbackWindow = 4;
+constexpr int kSweepTile = kSortThreads * kSweepItems;
+constexpr int kSweepSmem = kSweepTile * (sizeof(uint64_t) + sizeof(uint32_t));
+static_assert(kSweepTile >= 2048, "sweep_bytes() sizes the look-back words for 2048-key tiles");
+constexpr int kLookbackSpinLimit = 1 << 22;
+
+__device__ __forceinline__ void lb_store(uint64_t *p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t lb_load(const uint64_t *p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+template <bool IDENTITY_IN>
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t *__restrict__ kin,
+                                                           const uint32_t *__restrict__ vin,
+                                                           uint64_t *__restrict__ kout,
+                                                           uint32_t *__restrict__ vout,
+                                                           int64_t n, int shift,
+                                                           const uint32_t *__restrict__ hist,
+                                                           uint64_t *lookback,
+                                                           int32_t *tile_counter,
+                                                           int32_t *flags) {
+    static_assert(kSortThreads == 256, "block scans assume 256 threads");
+    constexpr int W = kSortThreads / 32;
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t *skey = reinterpret_cast<uint64_t *>(smem);
+    uint32_t *sval = reinterpret_cast<uint32_t *>(smem + kSweepTile * sizeof(uint64_t));
+    __shared__ uint32_t wcnt[W][257];
+    __shared__ uint32_t gbase[256];
+    __shared__ uint32_t tstart[256];
+    __shared__ uint32_t wsum[8];
+    __shared__ int s_tile;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // tiles in the order blocks start: every tile this one waits for has started
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1);
+    for (int i = threadIdx.x; i < W * 257; i += kSortThreads) (&wcnt[0][0])[i] = 0;
+    // start of each digit among all keys
+    const uint32_t digit_start = block_exscan256(hist[threadIdx.x], wsum);
+    __syncthreads();
+    const int64_t tile = s_tile;
+
+    const uint32_t lt_mask = (1u << lane) - 1u;
+    const int64_t tbase = tile * kSweepTile;
+    const int64_t wbase = tbase + (int64_t)warp * 32 * kSweepItems;
+    uint64_t key[kSweepItems];
+    uint32_t val[kSweepItems];
+    uint32_t rank[kSweepItems];
+    // every load of the tile in flight before the first is used
+#pragma unroll
+    for (int r = 0; r < kSweepItems; ++r) {
+        const int64_t e = wbase + r * 32 + lane;
+        key[r] = e < n ? __ldcs(kin + e) : 0;
+        val[r] = IDENTITY_IN ? (uint32_t)e : (e < n ? __ldcs(vin + e) : 0u);
+    }
+#pragma unroll
+    for (int r = 0; r < kSweepItems; ++r) {
+        const int64_t e = wbase + r * 32 + lane;
+        // sentinel digit 256 for lanes past the end
+        const uint32_t d = e < n ? (uint32_t)(key[r] >> shift) & 255u : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = wcnt[warp][d];
+        __syncwarp();
+        if ((peers & lt_mask) == 0) wcnt[warp][d] = before + __popc(peers);
+        __syncwarp();
+        rank[r] = before + __popc(peers & lt_mask);
+    }
+    __syncthreads();
+    {
+        const int d = threadIdx.x;
+        uint32_t run = 0;
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+            const uint32_t c = wcnt[w][d];
+            wcnt[w][d] = run;
+            run += c;
+        }
+        // publish this tile's count, then add up the earlier tiles' counts
+        uint64_t *mine = lookback + tile * 256 + d;
+        uint32_t before = 0;
+        if (tile == 0) {
+            lb_store(mine, kLbPrefix | run);
+        } else {
+            lb_store(mine, kLbCount | run);
+            // kLookbackWindow earlier tiles per round trip, used in order up
+            // to the first one not yet published (tile 0 always ends the walk)
+            int64_t j = tile - 1;
+            int spins = 0;
+            for (;;) {
+                uint64_t v[kLookbackWindow];
+#pragma unroll
+                for (int w = 0; w < kLookbackWindow; ++w)
+                    v[w] = (j - w >= 0) ? lb_load(lookback + (j - w) * 256 + d) : kLbPrefix;
+                int used = 0;
+                bool done = false;
+#pragma unroll
+                for (int w = 0; w < kLookbackWindow; ++w) {
+                    const uint32_t state = (uint32_t)(v[w] >> 32);
+                    if (!done && used == w && state != 0) {
+                        before += (uint32_t)v[w];
+                        used = w + 1;
+                        done = (state == 2);
+                    }
+                }
+                if (done) break;
+                j -= used;
+                if (used == 0) {
+                    if (++spins > kLookbackSpinLimit) {
+                        set_flag(flags, CNB_FLAG_WAIT_LIMIT);
+                        break;
+                    }
+                    if (spins > 16) __nanosleep(64);
+                }
+            }
+            lb_store(mine, kLbPrefix | (before + run));
+        }
+        gbase[d] = digit_start + before;
+        tstart[d] = block_exscan256(run, wsum);
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kSweepItems; ++r) {
+        const int64_t e = wbase + r * 32 + lane;
+        if (e < n) {
+            const uint32_t d = (uint32_t)(key[r] >> shift) & 255u;
+            const uint32_t lp = tstart[d] + wcnt[warp][d] + rank[r];
+            skey[lp] = key[r];
+            sval[lp] = val[r];
+        }
+    }
+    __syncthreads();
+    const int tile_n = (int)min((int64_t)kSweepTile, n - tbase);
+    for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
+        const uint64_t k = skey[j];
+        const uint32_t d = (uint32_t)(k >> shift) & 255u;
+        const int64_t pos = (int64_t)gbase[d] + (j - tstart[d]);
+        kout[pos] = k;
+        vout[pos] = sval[j];
+    }
+}
+
+__global__ void k_take_flags(int32_t *ctx_flags, int32_t *status) {
+    const int32_t f = *ctx_flags;
+    if (f) {
+        atomicOr(status, f);
+        *ctx_flags = 0;
+    }
+}
+
+int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
+                        const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
+                        cudaStream_t st) {
+    if (n == 0) return CNB_OK;
+    int passes = (key_bits + 7) / 8;
+    if (passes < 1) passes = 1;
+    if (passes == 1 && keys_in == keys_out) passes = 2;
+    const int64_t tiles = (n + kSweepTile - 1) / kSweepTile;
+    uint32_t *hist = ctx->sweep;
+    int32_t *counters = reinterpret_cast<int32_t *>(ctx->sweep + kSweepPasses * 256);
+    uint64_t *lookback = reinterpret_cast<uint64_t *>(ctx->sweep + kSweepMetaWords);
+    CNB_CUDA(cudaMemsetAsync(ctx->sweep, 0,
+                             kSweepMetaWords * 4 + (size_t)passes * tiles * 256 * 8, st));
+    CNB_CUDA(cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kSweepSmem));
+    CNB_CUDA(cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kSweepSmem));
+    k_digit_hist_all<<<grid_for(n, kSortTile, 148 * 8), kSortThreads, 0, st>>>(keys_in, n, passes,
+                                                                              hist);
+    CNB_TRY(launch_status());
+    const uint64_t *ks = keys_in;
+    const uint32_t *vs = idx_in;
+    for (int p = 0; p < passes; ++p) {
+        const bool last = (p == passes - 1);
+        uint64_t *kd = last ? keys_out : ctx->keys_tmp[p & 1];
+        uint32_t *vd = last ? perm_out : ctx->vals_tmp[p & 1];
+        uint64_t *lb = lookback + (int64_t)p * tiles * 256;
+        if (vs == nullptr)
+            k_onesweep<true><<<(unsigned)tiles, kSortThreads, kSweepSmem, st>>>(
+                ks, nullptr, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags);
+        else
+            k_onesweep<false><<<(unsigned)tiles, kSortThreads, kSweepSmem, st>>>(
+                ks, vs, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags);
+        CNB_TRY(launch_status());
+        ks = kd;
+        vs = vd;
+    }
+    return CNB_OK;
+}
+
 struct GatherArgs {
     const float *src[8];
     float *dst[8];
@@ -290,7 +536,9 @@ extern "C" int cnb_ctx_create(int64_t n_max, cnb_ctx **out) {
         e = cudaMalloc(&c->keys_tmp[k], sizeof(uint64_t) * nn);
         if (e == cudaSuccess) e = cudaMalloc(&c->vals_tmp[k], sizeof(uint32_t) * nn);
     }
-    if (e == cudaSuccess) e = cudaMalloc(&c->tile_hist, sizeof(uint32_t) * 256 * (c->tiles_max + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&c->sweep, cnb::sweep_bytes(nn));
+    if (e == cudaSuccess) e = cudaMalloc(&c->flags, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(c->flags, 0, sizeof(int32_t));
     if (e != cudaSuccess) {
         cnb_ctx_destroy(c);
         cnb::record_cuda_error(e);
@@ -307,6 +555,8 @@ extern "C" int cnb_ctx_destroy(cnb_ctx *c) {
         cudaFree(c->vals_tmp[k]);
     }
     cudaFree(c->tile_hist);
+    cudaFree(c->sweep);
+    cudaFree(c->flags);
     cudaFree(c->group_scratch);
     delete c;
     return CNB_OK;
@@ -318,8 +568,14 @@ extern "C" int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *k
     if (!ctx || n < 0 || key_bits < 1 || key_bits > 64) return CNB_E_INVALID_ARG;
     if (n > ctx->n_max) return CNB_E_TOO_LARGE;
     if (n > 0 && (!keys_in || !keys_out || !perm_out)) return CNB_E_INVALID_ARG;
-    return cnb::sort_pairs(ctx, keys_in, keys_out, idx_in, perm_out, n, key_bits,
-                           cnb::as_stream(stream));
+    return cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, idx_in, perm_out, n, key_bits,
+                                    cnb::as_stream(stream));
+}
+
+extern "C" int cnb_ctx_take_flags(cnb_ctx *ctx, int32_t *status, void *stream) {
+    if (!ctx || !status) return CNB_E_INVALID_ARG;
+    cnb::k_take_flags<<<1, 1, 0, cnb::as_stream(stream)>>>(ctx->flags, status);
+    return cnb::launch_status();
 }
 
 extern "C" int cnb_gather_f32(const uint32_t *perm, int n_arrays, const float *const *src,

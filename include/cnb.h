@@ -38,6 +38,7 @@ extern "C" {
 #define CNB_FLAG_BAD_TOPOLOGY 2   /* climb longer than the node count, or child index out of range */
 #define CNB_FLAG_NONFINITE 4      /* non-finite acceleration produced */
 #define CNB_FLAG_LIST_OVERFLOW 8  /* grouped traversal work queue exhausted */
+#define CNB_FLAG_WAIT_LIMIT 16    /* a bounded wait between blocks gave up (result invalid) */
 
 /* Morton key modes */
 #define CNB_KEY_COMPAT30 0 /* bit-exact with morton.py:13-63 (low 10 bits of each 21-bit coordinate) */
@@ -75,10 +76,19 @@ int cnb_ctx_destroy(cnb_ctx *ctx);
 /* src/core/state.py:35 `sort_idx = cp.argsort(codes)`: stable LSD radix
  * sort of (key, index) pairs.  keys_out receives the sorted keys, perm_out
  * the original index of each sorted key.  idx_in may be NULL (identity).
- * key_bits = number of low key bits that may be non-zero (30 or 63). */
+ * key_bits = number of low key bits that may be non-zero (30 or 63).
+ * One kernel per 8-bit digit: each 4096-key tile finds where its keys go by
+ * looking back at the counts earlier tiles publish; the waits are bounded,
+ * and a wait that gives up raises CNB_FLAG_WAIT_LIMIT in the context
+ * (cnb_ctx_take_flags). */
 int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                    const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
                    void *stream);
+
+/* No counterpart in the reference: ORs the flags the context's kernels
+ * raised into the caller's device status word and clears them (stream
+ * ordered, no synchronisation). */
+int cnb_ctx_take_flags(cnb_ctx *ctx, int32_t *status, void *stream);
 
 /* No counterpart in the reference.  The same stable (key, index) sort as
  * cnb_sort_pairs for callers that cannot allocate device memory (a plugin

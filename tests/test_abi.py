@@ -58,6 +58,7 @@ def test_host_only_entry_points():
     assert lib.cnb_forces_two_level(None, None, None, None, None, None, None, None, 0, 1024, None,
                                     5, 0.5, 1, 8, 1.0, 0.01, 1.0, None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_sort_pairs(None, None, None, None, None, 5, 30, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_ctx_take_flags(None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_render_density(None, None, None, None, None, 4, 0, 4, None) == _lib.CNB_E_INVALID_ARG
 
 

@@ -118,6 +118,65 @@ def test_sort_stable_bit_exact(n, bits):
     np.testing.assert_array_equal(sk, keys[want])
 
 
+@pytest.mark.parametrize("kind", ["random", "sorted", "nearly_sorted", "reversed", "few_values"])
+def test_sort_large_bit_exact_one_context(kind):
+    """Millions of keys, several sizes on one context (the look-back state is
+    reset by every call), every input order the step sees."""
+    rng = np.random.default_rng(11)
+    ctx = Ctx(5_000_000)
+    for n, bits in ((5_000_000, 63), (2_097_152, 64), (777_777, 30), (4096 * 3 + 5, 16)):
+        if kind == "few_values":
+            keys = rng.integers(0, 7, n, dtype=np.uint64) << np.uint64(max(bits - 3, 0))
+        else:
+            keys = rng.integers(0, 1 << 62, n, dtype=np.uint64) >> np.uint64(max(62 - bits, 0))
+            if bits == 64:
+                keys |= rng.integers(0, 2, n, dtype=np.uint64) << np.uint64(63)
+        if kind == "sorted":
+            keys = np.sort(keys)
+        elif kind == "reversed":
+            keys = np.sort(keys)[::-1].copy()
+        elif kind == "nearly_sorted":
+            keys = np.sort(keys)
+            sw = rng.integers(0, n - 1, n // 50)
+            keys[sw], keys[sw + 1] = keys[sw + 1].copy(), keys[sw].copy()
+        K = dev(keys)
+        Ko = torch.zeros_like(K)
+        P = torch.zeros(n, dtype=torch.uint32, device="cuda")
+        lib().call("cnb_sort_pairs", ctx.p, K.data_ptr(), Ko.data_ptr(), None, P.data_ptr(), n, bits,
+                   stream())
+        want = np.argsort(keys, kind="stable")
+        np.testing.assert_array_equal(host(P).astype(np.int64), want)
+        np.testing.assert_array_equal(host(Ko), keys[want])
+    flags = torch.zeros(1, dtype=torch.int32, device="cuda")
+    lib().call("cnb_ctx_take_flags", ctx.p, flags.data_ptr(), stream())
+    assert int(host(flags)[0]) == 0
+
+
+def test_sort_replays_in_a_cuda_graph():
+    rng = np.random.default_rng(12)
+    n = 1_000_003
+    keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
+    ctx = Ctx(n)
+    K = dev(keys)
+    Ko = torch.zeros_like(K)
+    P = torch.zeros(n, dtype=torch.uint32, device="cuda")
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        st = int(s.cuda_stream)
+        lib().call("cnb_sort_pairs", ctx.p, K.data_ptr(), Ko.data_ptr(), None, P.data_ptr(), n, 63, st)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=s):
+            lib().call("cnb_sort_pairs", ctx.p, K.data_ptr(), Ko.data_ptr(), None, P.data_ptr(), n, 63,
+                       int(s.cuda_stream))
+    torch.cuda.current_stream().wait_stream(s)
+    want = np.argsort(keys, kind="stable")
+    for _ in range(3):
+        P.zero_()
+        g.replay()
+        np.testing.assert_array_equal(host(P).astype(np.int64), want)
+
+
 def test_sort_all_equal_and_carried_values():
     n = 20000
     keys = np.full(n, 12345, np.uint64)
