@@ -84,6 +84,9 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
                                            const float (&y)[BPL], const float (&z)[BPL],
                                            float soft2, float (&ax)[BPL], float (&ay)[BPL],
                                            float (&az)[BPL]) {
+    // the softening enters the distance chain (d^2 + eps^2 in three FMAs);
+    // the reference's cut d^2 > 1e-7 becomes d^2 + eps^2 > eps^2 + 1e-7
+    const float cut = soft2 + 1e-7f;
 #pragma unroll 4
     for (int j = 0; j < cnt; ++j) {
         const float4 e = list[j];
@@ -95,9 +98,9 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
                 dy -= image_of(dy);
                 dz -= image_of(dz);
             }
-            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-            const float r = rsqrtf(d2 + soft2);
-            const float f = (d2 > 1e-7f) ? e.w * r * r * r : 0.f;
+            const float q = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
+            const float r = rsqrtf(q);
+            const float f = (q > cut) ? e.w * r * r * r : 0.f;
             ax[b] = fmaf(f, dx, ax[b]);
             ay[b] = fmaf(f, dy, ay[b]);
             az[b] = fmaf(f, dz, az[b]);
@@ -120,6 +123,7 @@ __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, con
     const float2 nx = make_float2(-x[0], -x[1]), ny = make_float2(-y[0], -y[1]),
                  nz = make_float2(-z[0], -z[1]);
     const float2 s2 = make_float2(soft2, soft2);
+    const float cut = soft2 + 1e-7f;  // the reference's d^2 > 1e-7 on d^2 + eps^2
     const float2 rc = make_float2(12582912.f, 12582912.f), nrc = make_float2(-12582912.f, -12582912.f);
     const float2 m1 = make_float2(-1.f, -1.f);
     float2 fx = make_float2(ax[0], ax[1]), fy = make_float2(ay[0], ay[1]),
@@ -141,15 +145,15 @@ __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, con
                 dy[u] = __ffma2_rn(__fadd2_rn(__fadd2_rn(dy[u], rc), nrc), m1, dy[u]);
                 dz[u] = __ffma2_rn(__fadd2_rn(__fadd2_rn(dz[u], rc), nrc), m1, dz[u]);
             }
-            d2[u] = __ffma2_rn(dx[u], dx[u], __ffma2_rn(dy[u], dy[u], __fmul2_rn(dz[u], dz[u])));
+            d2[u] = __ffma2_rn(dx[u], dx[u], __ffma2_rn(dy[u], dy[u], __ffma2_rn(dz[u], dz[u], s2)));
         }
         float2 f[8];
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
-            const float2 q = __fadd2_rn(d2[u], s2);
+            const float2 q = d2[u];
             float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
-            r0 = d2[u].x > 1e-7f ? r0 : 0.f;
-            r1 = d2[u].y > 1e-7f ? r1 : 0.f;
+            r0 = q.x > cut ? r0 : 0.f;
+            r1 = q.y > cut ? r1 : 0.f;
             const float2 r = make_float2(r0, r1);
             f[u] = __fmul2_rn(__fmul2_rn(__fmul2_rn(w[u], r), r), r);
         }
@@ -170,11 +174,10 @@ __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, con
             dy = __ffma2_rn(__fadd2_rn(__fadd2_rn(dy, rc), nrc), m1, dy);
             dz = __ffma2_rn(__fadd2_rn(__fadd2_rn(dz, rc), nrc), m1, dz);
         }
-        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
-        const float2 q = __fadd2_rn(d2, s2);
+        const float2 q = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
         float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
-        r0 = d2.x > 1e-7f ? r0 : 0.f;
-        r1 = d2.y > 1e-7f ? r1 : 0.f;
+        r0 = q.x > cut ? r0 : 0.f;
+        r1 = q.y > cut ? r1 : 0.f;
         const float2 r = make_float2(r0, r1);
         const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(b.z, b.w), r), r), r);
         fx = __ffma2_rn(f, dx, fx);

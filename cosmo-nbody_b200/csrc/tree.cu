@@ -176,20 +176,23 @@ __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
             reinterpret_cast<float4 *>(n_err)[i] = make_float4(a.em, a.ex, a.ey, a.ez);
         }
         int64_t curr = i;
+        int32_t p = parents[curr];
         for (int64_t guard = 0;; ++guard) {
             if (guard > m_nodes) {
                 set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
                 break;
             }
-            const int32_t p = parents[curr];
             if (p == -1) break;
             if (p < 0 || p >= m_nodes) {
                 set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
                 break;
             }
+            // this level's and the next level's topology are read while the
+            // counter's atomic is in flight (they do not depend on it)
+            const int32_t l = __ldg(children + 2 * p), r = __ldg(children + 2 * p + 1);
+            const int32_t pp = __ldg(parents + p);
             // release this node's data, acquire the sibling's: the first arrival stops
             if (atomic_add_acq_rel(counts + p, 1) == 0) break;
-            const int32_t l = children[2 * p], r = children[2 * p + 1];
             const bool mine_left = (l == curr);
             const int32_t s = mine_left ? r : l;
             if ((!mine_left && r != curr) || s == curr || s < 0 || s >= m_nodes) {
@@ -244,6 +247,7 @@ __global__ void __launch_bounds__(256) k_upward(const float *__restrict__ px,
             n_max[3 * p + 2] = q.hz;
             a = q;
             curr = p;
+            p = pp;
         }
     }
 }

@@ -53,20 +53,23 @@ __global__ void __launch_bounds__(256) k_upward_table(
         sums[i] = s;
         store_record(rec, aabb, i, s, lo, hi, -1, -1);
         int64_t curr = i;
+        int32_t p = parents[curr];
         for (int64_t guard = 0;; ++guard) {
             if (guard > m_nodes) {
                 set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
                 break;
             }
-            const int32_t p = parents[curr];
             if (p == -1) break;
             if (p < 0 || p >= m_nodes) {
                 set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
                 break;
             }
+            // the topology of this level and the next is read while the
+            // counter's atomic is in flight (it does not depend on it)
+            const int2 ch = __ldg(children + p);
+            const int32_t pp = __ldg(parents + p);
             // release this node's data, acquire the sibling's: the first arrival stops
             if (atomic_add_acq_rel(counts + p, 1) == 0) break;
-            const int2 ch = children[p];
             const bool mine_left = (ch.x == curr);
             const int32_t sib = mine_left ? ch.y : ch.x;
             if ((!mine_left && ch.y != curr) || sib == curr || sib < 0 || sib >= m_nodes) {
@@ -91,6 +94,7 @@ __global__ void __launch_bounds__(256) k_upward_table(
             lo = qlo;
             hi = qhi;
             curr = p;
+            p = pp;
         }
     }
 }
