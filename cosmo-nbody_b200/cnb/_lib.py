@@ -29,6 +29,7 @@ KEY_COMPAT30 = 0
 KEY_MORTON63 = 1
 MAC_REF_X = 0
 MAC_PERIODIC = 1
+MAC_EWALD = 2
 PREC_F32 = 0
 PREC_F64 = 1
 UPWARD_PLAIN = 0
@@ -90,6 +91,10 @@ SIGNATURES = {
     "cnb_adam_step": (_int, [_p, _p, _p, _p, _int, _f, _f, _f, _f, _int, _p]),
     "cnb_to_bf16": (_int, [_p, _p, _int, _p]),
     "cnb_colorize": (_int, [_p, _int, _int, _p, _p, _p, _p]),
+    "cnb_ewald_table": (_int, [_p, _int, _p]),
+    "cnb_forces_grouped_ewald": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _d, _d, _p,
+                                        _int, _p, _p, _p]),
+    "cnb_direct_sum_ewald_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_direct_sum_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_fma_probe": (_int, [_p, _i64, _int, _p]),
 }

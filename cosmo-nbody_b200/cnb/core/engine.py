@@ -11,7 +11,8 @@ kernel is chosen by config.FORCE_MODE:
                test (config.PRECISION "f64" = the reference's arithmetic,
                "f32" = float32);
   "grouped"    warp-per-bucket traversal (config.MAC "ref_x" or "periodic",
-               optional per-bucket theta from `theta_per_group`); with
+               optional per-bucket theta from `theta_per_group`; "ewald" = the
+               periodic force law, not the reference's minimum image); with
                config.SUPER_BODIES > 0 and the "ref_x" test, the two-level
                form (super-buckets of that many bodies walk the top of the
                tree once for all their buckets).
@@ -28,7 +29,8 @@ from ..utils.cosmology import get_hubble_param
 from .camera import Camera
 from .octree import OctreeManager
 
-MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC}
+MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC, "ewald": _lib.MAC_EWALD}
+EWALD_NT = 64   # Ewald correction table: 65^3 points on [0, 1/2]^3
 
 
 class SimulationEngine:
@@ -62,6 +64,13 @@ class SimulationEngine:
         # periodic test: image-ambiguous nodes of at most SLAB_BODIES bodies' mass are applied
         # with the per-pair minimum image (0 = exact)
         self.slab_mass = float(getattr(config, "SLAB_BODIES", 0)) / max(state.n, 1)
+        self.ewald_table = None
+        if self.mac == _lib.MAC_EWALD:
+            if self.force_mode != "grouped":
+                raise ValueError("MAC 'ewald' needs FORCE_MODE 'grouped'")
+            self.ewald_table = torch.empty(((EWALD_NT + 1) ** 3, 12), dtype=torch.float32,
+                                           device=state.device)
+            _lib.call("cnb_ewald_table", self.ewald_table.data_ptr(), EWALD_NT, self._stream())
         self.super_bodies = 0
         self.super_ws = None
         if self.force_mode == "grouped":
@@ -102,6 +111,13 @@ class SimulationEngine:
                     tm.node_table, tm.parent, tm.workspace, s.n, out=self.theta_per_group,
                     scale=self.controller_scale)
             tpg = self.theta_per_group
+            if self.ewald_table is not None:
+                _lib.call("cnb_forces_grouped_ewald", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                          tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,
+                          float(cfg.THETA), tpg.data_ptr() if tpg is not None else None,
+                          self.bodies_per_lane, self.block_warps, float(cfg.G), float(cfg.SOFTENING),
+                          self.ewald_table.data_ptr(), EWALD_NT, self.stats.data_ptr(), status, st)
+                return
             if self.super_ws is not None and tpg is None:
                 _lib.call("cnb_forces_two_level", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                           tm.node_table.data_ptr(), tm.ranges.data_ptr(), tm.parent.data_ptr(),

@@ -38,7 +38,8 @@ STACK_SIZE_CHILD = 128
 # --- B200 step options (no reference counterpart) ---
 KEY_MODE = "compat30"      # "compat30": reference keys, bit-exact; "morton63": full 21-bit interleave
 FORCE_MODE = "reference"   # "reference": per-particle stack traversal; "grouped": warp-per-bucket traversal
-MAC = "ref_x"              # "ref_x": reference opening test; "periodic": 3-D extent + image-safe opening
+MAC = "ref_x"              # "ref_x": reference opening test; "periodic": 3-D extent + image-safe opening;
+                           # "ewald": periodic (Ewald) force law instead of the minimum image, 3-D extent
 PRECISION = "f32"          # per-particle traversal arithmetic: "f32" or "f64" (the reference's)
 UPWARD = "plain"           # "plain": bit-exact upward pass; "compensated": two-sum + float64 root
 BODIES_PER_LANE = 1        # grouped traversal: bodies per lane (buckets of 32 x this)

@@ -67,7 +67,40 @@ struct GroupedParams {
                                    // front, per-pair ones from the back
     const int32_t *near_lists;     // per super-bucket: near_cap nodes left to each bucket
     int far_cap, near_cap;
+    // CNB_MAC_EWALD: g and its Jacobian on the octant grid (cnb_ewald_table)
+    const float4 *ewald;
+    int ewald_nt;
 };
+
+// Periodic correction of one accepted node, d = its CoM image minus the
+// bucket centre (|d_i| <= 1/2): g(d) and its Jacobian from the nearest
+// point of the octant table, g to first order about that point, signs from
+// g's symmetry (g_i odd in d_i, even in the other components).
+__device__ __forceinline__ void ewald_lookup(const float4 *__restrict__ T, int nt, float dx,
+                                             float dy, float dz, float (&g)[3], float (&J)[6]) {
+    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+    const float sc = 2.f * nt;
+    const int i = min(__float2int_rn(ax * sc), nt), j = min(__float2int_rn(ay * sc), nt),
+              k = min(__float2int_rn(az * sc), nt);
+    const int64_t t = ((int64_t)i * (nt + 1) + j) * (nt + 1) + k;
+    const float4 t0 = __ldg(T + 3 * t), t1 = __ldg(T + 3 * t + 1), t2 = __ldg(T + 3 * t + 2);
+    const float h = 1.f / sc;
+    const float ex = ax - i * h, ey = ay - j * h, ez = az - k * h;
+    // octant: g(a) = g(a0) + J(a0) (a - a0); J = (xx, xy, xz, yy, yz, zz)
+    const float gx = t0.x + t1.x * ex + t1.y * ey + t1.z * ez;
+    const float gy = t0.y + t1.y * ex + t1.w * ey + t2.x * ez;
+    const float gz = t0.z + t1.z * ex + t2.x * ey + t2.y * ez;
+    const float sx = dx < 0.f ? -1.f : 1.f, sy = dy < 0.f ? -1.f : 1.f, sz = dz < 0.f ? -1.f : 1.f;
+    g[0] = sx * gx;
+    g[1] = sy * gy;
+    g[2] = sz * gz;
+    J[0] = t1.x;
+    J[1] = sx * sy * t1.y;
+    J[2] = sx * sz * t1.z;
+    J[3] = t1.w;
+    J[4] = sy * sz * t2.x;
+    J[5] = t2.y;
+}
 
 // Nearest-image offset of a coordinate difference d with |d| < 1.5:
 // -1, 0 or +1, equal to rint(d) there (ties at +-0.5 round to 0, as rint
@@ -219,7 +252,7 @@ constexpr size_t grouped_smem(int warps) {
                             2 * kGList * entry_width<BPL>() * sizeof(float4));
 }
 
-template <int BPL, int WARPS>
+template <int BPL, int WARPS, bool EWALD>
 __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) {
     extern __shared__ __align__(16) unsigned char g_smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
@@ -293,6 +326,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
         float ax[BPL], ay[BPL], az[BPL];
 #pragma unroll
         for (int b = 0; b < BPL; ++b) ax[b] = ay[b] = az[b] = 0.f;
+        // EWALD: this lane's share of sum m (c - centre), sum m, sum m g, sum m J
+        float ec[4] = {0.f, 0.f, 0.f, 0.f}, eg[3] = {0.f, 0.f, 0.f};
+        float ej[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         int top = 1, cnt = 0, wcnt = 0;
         unsigned long long n_entries = 0, n_wrap = 0;
         bool seeded = false;
@@ -366,7 +402,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                         const float ty = fmaxf(fabsf(dy) - ghy, 0.f);
                         const float tz = fmaxf(fabsf(dz) - ghz, 0.f);
                         const float d2min = tx * tx + ty * ty + tz * tz;
-                        if (P.mac == CNB_MAC_REF_X) {
+                        if (EWALD) {
+                            // periodic law: every image is valid, the 3-D extent decides
+                            accept = S.y * S.y < th2 * d2min;
+                        } else if (P.mac == CNB_MAC_REF_X) {
                             const float s = S.x > half_box ? P.box : S.x;
                             accept = s * s < th2 * d2min;
                         } else if (S.y * S.y < th2 * d2min) {
@@ -384,9 +423,22 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                         open = !accept;
                     }
                     if (accept) {
-                        const bool same_image = consistent &&
-                            fabsf(dx) < wlx && fabsf(dy) < wly && fabsf(dz) < wlz;
+                        // under the periodic law one image serves the whole bucket
+                        const bool same_image = EWALD || (consistent &&
+                            fabsf(dx) < wlx && fabsf(dy) < wly && fabsf(dz) < wlz);
                         E = make_float4(A.x - sx_, A.y - sy_, A.z - sz_, same_image ? A.w : -A.w);
+                        if (EWALD) {
+                            float g[3], J[6];
+                            ewald_lookup(P.ewald, P.ewald_nt, dx, dy, dz, g, J);
+                            ec[0] = fmaf(A.w, dx, ec[0]);
+                            ec[1] = fmaf(A.w, dy, ec[1]);
+                            ec[2] = fmaf(A.w, dz, ec[2]);
+                            ec[3] += A.w;
+#pragma unroll
+                            for (int q = 0; q < 3; ++q) eg[q] = fmaf(A.w, g[q], eg[q]);
+#pragma unroll
+                            for (int q = 0; q < 6; ++q) ej[q] = fmaf(A.w, J[q], ej[q]);
+                        }
                     }
                 }
             }
@@ -444,6 +496,31 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
         n_entries += cnt + wcnt;
         n_wrap += wcnt;
         __syncwarp();
+        if (EWALD) {
+            // bucket totals, then per body the periodic correction of every
+            // accepted node: -(4 pi/3) sum m (c - x) + sum m g(c - centre)
+            // + sum m J(c - centre) (centre - x)
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                for (int q = 0; q < 4; ++q) ec[q] += __shfl_xor_sync(0xffffffffu, ec[q], o);
+#pragma unroll
+                for (int q = 0; q < 3; ++q) eg[q] += __shfl_xor_sync(0xffffffffu, eg[q], o);
+#pragma unroll
+                for (int q = 0; q < 6; ++q) ej[q] += __shfl_xor_sync(0xffffffffu, ej[q], o);
+            }
+            const float lin = 4.18879020478639f;  // 4 pi / 3
+#pragma unroll
+            for (int b = 0; b < BPL; ++b) {
+                const float ux = gcx - x[b], uy = gcy - y[b], uz = gcz - z[b];
+                // sum m (c - x) = sum m (c - centre) + M (centre - x)
+                const float cx = fmaf(ec[3], ux, ec[0]), cy = fmaf(ec[3], uy, ec[1]),
+                            cz = fmaf(ec[3], uz, ec[2]);
+                ax[b] += eg[0] + ej[0] * ux + ej[1] * uy + ej[2] * uz - lin * cx;
+                ay[b] += eg[1] + ej[1] * ux + ej[3] * uy + ej[4] * uz - lin * cy;
+                az[b] += eg[2] + ej[2] * ux + ej[4] * uy + ej[5] * uz - lin * cz;
+            }
+        }
 #pragma unroll
         for (int b = 0; b < BPL; ++b) {
             if (valid[b]) {
@@ -661,29 +738,30 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
     return launch_status();
 }
 
-template <int BPL, int WARPS>
+template <int BPL, int WARPS, bool EWALD>
 static int launch_shape(GroupedParams &P, cudaStream_t st) {
     const size_t smem = grouped_smem<BPL>(WARPS);
-    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS>,
+    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS, EWALD>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS>, WARPS * 32,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS, EWALD>, WARPS * 32,
                                                   smem);
     // persistent grid: the work counter hands out buckets
-    k_forces_grouped<BPL, WARPS><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
+    k_forces_grouped<BPL, WARPS, EWALD><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
     return launch_status();
 }
 
 static int launch_grouped(GroupedParams &P, int bodies_per_lane, int block_warps,
                           cudaStream_t st) {
     CNB_CUDA(cudaMemsetAsync(P.ws + 1, 0, 2 * sizeof(int32_t), st));
+    const bool ew = (P.mac == CNB_MAC_EWALD);
     switch (bodies_per_lane * 16 + block_warps) {
-        case 16 + 2: return launch_shape<1, 2>(P, st);
-        case 16 + 4: return launch_shape<1, 4>(P, st);
-        case 16 + 8: return launch_shape<1, 8>(P, st);
-        case 32 + 2: return launch_shape<2, 2>(P, st);
-        case 32 + 4: return launch_shape<2, 4>(P, st);
-        case 32 + 8: return launch_shape<2, 8>(P, st);
+        case 16 + 2: return ew ? launch_shape<1, 2, true>(P, st) : launch_shape<1, 2, false>(P, st);
+        case 16 + 4: return ew ? launch_shape<1, 4, true>(P, st) : launch_shape<1, 4, false>(P, st);
+        case 16 + 8: return ew ? launch_shape<1, 8, true>(P, st) : launch_shape<1, 8, false>(P, st);
+        case 32 + 2: return ew ? launch_shape<2, 2, true>(P, st) : launch_shape<2, 2, false>(P, st);
+        case 32 + 4: return ew ? launch_shape<2, 4, true>(P, st) : launch_shape<2, 4, false>(P, st);
+        case 32 + 8: return ew ? launch_shape<2, 8, true>(P, st) : launch_shape<2, 8, false>(P, st);
         default: return CNB_E_INVALID_ARG;
     }
 }
@@ -828,6 +906,28 @@ extern "C" int cnb_forces_two_level(const float *px, const float *py, const floa
     P.far_cap = kFarCap;
     P.near_cap = kNearCap;
     return launch_grouped(P, bodies_per_lane, block_warps, st);
+}
+
+extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const float *pz,
+                                        const float *node_table, int32_t *workspace, float *force,
+                                        int64_t n, double theta, const float *theta_per_bucket,
+                                        int bodies_per_lane, int block_warps, double G, double soft,
+                                        const float *ewald_table, int ewald_nt,
+                                        unsigned long long *stats, int32_t *status, void *stream) {
+    GroupedParams P;
+    CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket,
+                           CNB_MAC_REF_X, bodies_per_lane, block_warps, G, stats, status));
+    if (n == 0) return CNB_OK;
+    if (!ewald_table || ewald_nt < 2 || ewald_nt > 512 ||
+        (reinterpret_cast<uintptr_t>(ewald_table) & 15))
+        return CNB_E_INVALID_ARG;
+    P.mac = CNB_MAC_EWALD;
+    P.theta = (float)theta;
+    P.soft2 = (float)(soft * soft);
+    P.box = 1.0f;
+    P.ewald = reinterpret_cast<const float4 *>(ewald_table);
+    P.ewald_nt = ewald_nt;
+    return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }
 
 extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,

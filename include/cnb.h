@@ -47,6 +47,7 @@ extern "C" {
 /* opening criteria */
 #define CNB_MAC_REF_X 0    /* physics_kernels.py:131-136: x-extent, clamped to box when > box/2 */
 #define CNB_MAC_PERIODIC 1 /* 3-D extent, and open any node whose image is ambiguous for a target */
+#define CNB_MAC_EWALD 2    /* periodic (Ewald) force law, 3-D extent: cnb_forces_grouped_ewald */
 
 /* arithmetic of the per-particle traversal */
 #define CNB_PREC_F32 0
@@ -265,6 +266,37 @@ int cnb_forces_two_level(const float *px, const float *py, const float *pz,
                          int super_bodies, float *force, int64_t n, double theta,
                          int bodies_per_lane, int block_warps, double G, double soft, double box,
                          unsigned long long *stats, int32_t *status, void *stream);
+
+/* ---- periodic (Ewald) force law (no reference counterpart; the reference
+ * applies the minimum-image force of physics_kernels.py:118-141) ----
+ * Unit box, d = source - target: the acceleration towards a point mass and
+ * all its images (neutralising background) is f_per(d) = d/|d|^3 -
+ * (4 pi/3) d + g(d), g smooth and O(|d|^3).
+ *
+ * Tabulates g and its Jacobian on the octant [0, 1/2]^3, (nt + 1)^3 points
+ * of spacing 1/(2 nt), computed in float64: table is float32
+ * [(nt + 1)^3, 12] (16-byte aligned), 2 <= nt <= 512. */
+int cnb_ewald_table(float *table, int nt, void *stream);
+
+/* cnb_forces_grouped under the periodic law: nodes open on their 3-D extent
+ * (l^2 < theta^2 dmin^2), one image of every accepted node serves the whole
+ * bucket, each body gets the softened monopoles plus, for every accepted
+ * node, -(4 pi/3) m (c - x) + m g(c - centre) + m J(c - centre) (centre - x)
+ * with g, J from the table of cnb_ewald_table. */
+int cnb_forces_grouped_ewald(const float *px, const float *py, const float *pz,
+                             const float *node_table, int32_t *workspace, float *force, int64_t n,
+                             double theta, const float *theta_per_bucket, int bodies_per_lane,
+                             int block_warps, double G, double soft, const float *ewald_table,
+                             int ewald_nt, unsigned long long *stats, int32_t *status,
+                             void *stream);
+
+/* Float64 periodic direct sum for the bodies listed in targets (accuracy
+ * oracle of the periodic law): per pair the softened monopole at the minimum
+ * image plus f_per - d/|d|^3, with the Ewald sums carried to float64
+ * precision.  out is float64 [n_targets, 3]. */
+int cnb_direct_sum_ewald_f64(const float *px, const float *py, const float *pz,
+                             const float *mass, int64_t n, const int64_t *targets,
+                             int64_t n_targets, double G, double soft, double *out, void *stream);
 
 /* src/utils/visualizer.py:115-171 colorize_frame (+ the 8-bit packing of
  * src/core/engine.py:139): grid [height, width] float32 -> rgb float32
