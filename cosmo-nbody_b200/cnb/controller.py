@@ -149,11 +149,13 @@ def bucket_features(node_table, parents, workspace, n):
     return out[:nb]
 
 
-def direct_sum(pos, mass, targets, G, soft):
-    """float64 minimum-image direct sum (libcnb) for `targets` of one box."""
+def direct_sum(pos, mass, targets, G, soft, periodic=False):
+    """float64 direct sum (libcnb) for `targets` of one box: the minimum-image
+    force law, or with `periodic` the periodic (Ewald) law."""
     T = targets.to(torch.int64).contiguous()
     out = torch.empty((T.numel(), 3), dtype=torch.float64, device=pos[0].device)
-    _lib.call("cnb_direct_sum_f64", *(p.data_ptr() for p in pos), mass.data_ptr(), pos[0].numel(),
+    _lib.call("cnb_direct_sum_ewald_f64" if periodic else "cnb_direct_sum_f64",
+              *(p.data_ptr() for p in pos), mass.data_ptr(), pos[0].numel(),
               T.data_ptr(), T.numel(), float(G), float(soft), out.data_ptr(), _st())
     return out
 
@@ -164,7 +166,8 @@ def make_labels(bb: BatchedBoxes, theta_grid=THETA_GRID, budget=None, per_box=48
 
     For every theta of the grid the plain traversal runs with that theta in
     every bucket; each sampled bucket's error is the largest force error of
-    its bodies against the float64 direct sum of its box, either relative to
+    its bodies against the float64 direct sum of its box (under the box's
+    force law: minimum image, or periodic for the "ewald" test), either relative to
     the body's own acceleration (error="relative") or to the box's RMS
     acceleration (error="rms").  The label is the largest theta whose error
     is within `budget`; budget None means the 99th-percentile error of plain
@@ -192,7 +195,8 @@ def make_labels(bb: BatchedBoxes, theta_grid=THETA_GRID, budget=None, per_box=48
         sl = bb.box_slice(b)
         local = torch.from_numpy(t - sl.start).to(bb.device)
         soft = 0.5 / bb.boxes[b]["n_grid"]
-        ref.append(direct_sum([p[sl] for p in bb.pos], bb.mass[sl], local, bb.G, soft))
+        ref.append(direct_sum([p[sl] for p in bb.pos], bb.mass[sl], local, bb.G, soft,
+                              periodic=bb.mac == _lib.MAC_EWALD))
         bodies.append(t)
         owner.append(o)
     box_rms = [r.norm(dim=1).pow(2).mean().sqrt().expand(r.shape[0]) for r in ref]

@@ -27,7 +27,8 @@ from .._arrays import check_status, status_buffer
 from ..utils.cosmology import zeldovich_arrays
 from .state import SortContext
 
-MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC}
+MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC, "ewald": _lib.MAC_EWALD}
+EWALD_NT = 64
 
 
 def draw_boxes(n_boxes=64, seed=3, grids=(16, 24, 32, 48, 64), a_range=(0.02, 0.1),
@@ -108,6 +109,11 @@ class BatchedBoxes:
         self.force = z(n, 3)
         self.stats = z(4, dt=torch.int64)
         self.theta_per_bucket = None
+        self.ewald_table = None
+        if self.mac == _lib.MAC_EWALD:
+            # every box is periodic on its own unit cube: one correction table serves all
+            self.ewald_table = z((EWALD_NT + 1) ** 3, 12)
+            _lib.call("cnb_ewald_table", self.ewald_table.data_ptr(), EWALD_NT, self._st())
         self._ctx = SortContext(n)
         self._graph = None
 
@@ -153,6 +159,15 @@ class BatchedBoxes:
         st = self._st()
         tpb = theta_per_bucket if theta_per_bucket is not None else self.theta_per_bucket
         p = self.pos
+        if self.ewald_table is not None:
+            _lib.call("cnb_forces_grouped_boxes_ewald", p[0].data_ptr(), p[1].data_ptr(),
+                      p[2].data_ptr(), self.table.data_ptr(), self.workspace.data_ptr(),
+                      self.force.data_ptr(), self.n, self.codes_sorted.data_ptr(), self.box_bits,
+                      self.box_roots.data_ptr(), self.box_params.data_ptr(),
+                      tpb.data_ptr() if tpb is not None else None, self.bpl, self.block_warps, self.G,
+                      self.ewald_table.data_ptr(), EWALD_NT, self.stats.data_ptr(),
+                      status_buffer(self.device.index).data_ptr(), st)
+            return
         _lib.call("cnb_forces_grouped_boxes", p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(),
                   self.table.data_ptr(), self.workspace.data_ptr(), self.force.data_ptr(), self.n,
                   self.codes_sorted.data_ptr(), self.box_bits, self.box_roots.data_ptr(),

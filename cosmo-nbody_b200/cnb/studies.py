@@ -2,7 +2,7 @@
 
     python -m cnb.studies precision   [--n-grid 256] [--steps 50]
     python -m cnb.studies batched     [--boxes 64] [--steps 10]
-    python -m cnb.studies controller  [--n-grid 128] [--evolve 100]
+    python -m cnb.studies controller  [--n-grid 128] [--evolve 100] [--mac ewald]
 
 precision:  Zel'dovich n^3 (seed 2) evolved `steps` kick-drift steps from
             a = 0.02 with da = 0.002; then, for theta in {0.3, 0.5, 0.7}, both
@@ -16,7 +16,9 @@ batched:    64 boxes, n drawn from {16, 24, 32, 48, 64}^3 (seed 3), a_start in
             same boxes stepped one by one.
 controller: labels from the batched boxes, training on the GPU, and learned
             theta against plain theta = 0.5 at matched 99th-percentile error
-            on an evolved n^3 state (seed 4).
+            on an evolved n^3 state (seed 4); under the minimum-image law with
+            the exact periodic test (default), or with --mac ewald under the
+            periodic (Ewald) law, each against its own float64 direct sum.
 Each prints one JSON object per configuration.
 """
 from __future__ import annotations
@@ -54,10 +56,11 @@ def _evolve(n_grid, seed, steps):
     return [p.clone() for p in eng.state.pos], [v.clone() for v in eng.state.vel], eng.a
 
 
-def _direct(state, targets, soft):
+def _direct(state, targets, soft, periodic=False):
     T = torch.from_numpy(targets).cuda()
     out = torch.empty((targets.size, 3), dtype=torch.float64, device="cuda")
-    _lib.call("cnb_direct_sum_f64", *(p.data_ptr() for p in state.pos), state.mass.data_ptr(), state.n,
+    _lib.call("cnb_direct_sum_ewald_f64" if periodic else "cnb_direct_sum_f64",
+              *(p.data_ptr() for p in state.pos), state.mass.data_ptr(), state.n,
               T.data_ptr(), targets.size, 1.0, float(soft), out.data_ptr(),
               int(torch.cuda.current_stream().cuda_stream))
     return out
@@ -206,19 +209,22 @@ def batched(args):
 def controller(args):
     from .controller import ThetaController, make_labels
     t0 = time.time()
-    train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac="periodic")
+    law = "ewald" if args.mac == "ewald" else "periodic"
+    train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac=law, bodies_per_lane=args.bpl)
     X, y, info = make_labels(train, per_box=args.per_box, error=args.error)
     del train
     ctl = ThetaController(seed=0)
     curve = ctl.train(X, y, steps=args.train_steps, lr=3e-3, over_weight=4.0)
     pos, vel, a = _evolve(args.n_grid, 4, args.evolve)
     n = args.n_grid ** 3
-    cfg = _cfg(args.n_grid, MAC="periodic")
+    cfg = _cfg(args.n_grid, MAC=law, BODIES_PER_LANE=args.bpl)
     st = SimulationState(n, pos, vel)
     eng = SimulationEngine(cfg, st, camera=False)
     eng.forces_only()
-    targets = np.sort(np.random.default_rng(0).choice(n, 4096, replace=False)).astype(np.int64)
-    ref = _direct(st, targets, cfg.SOFTENING)
+    # the periodic oracle costs hundreds of float64 terms per pair: fewer targets
+    n_t = 4096 if law == "periodic" else 1024
+    targets = np.sort(np.random.default_rng(0).choice(n, n_t, replace=False)).astype(np.int64)
+    ref = _direct(st, targets, cfg.SOFTENING, periodic=law == "ewald")
     key = "p99_rms" if args.error == "rms" else "p99_rel"
 
     def run(scale=None):
@@ -245,7 +251,7 @@ def controller(args):
     learned = run(lo)
     eng.controller = None
     eng.check()
-    print(json.dumps(dict(study="controller", n_grid=args.n_grid, evolve_steps=args.evolve, a=a,
+    print(json.dumps(dict(study="controller", law=law, n_grid=args.n_grid, evolve_steps=args.evolve, a=a,
                           error=args.error, labels=info, train_loss=[curve[0], curve[-1]],
                           plain_theta05=plain, learned=learned, learned_scale=lo,
                           speedup_forces=plain["ms"] / learned["ms"],
@@ -263,6 +269,7 @@ def main():
     ap.add_argument("--per-box", type=int, default=48)
     ap.add_argument("--train-steps", type=int, default=1500)
     ap.add_argument("--error", default="rms", choices=["rms", "relative"])
+    ap.add_argument("--bpl", type=int, default=1, choices=[1, 2])
     args = ap.parse_args()
     if args.study == "precision":
         args.n_grid = args.n_grid or 256

@@ -930,6 +930,35 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
     return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }
 
+extern "C" int cnb_forces_grouped_boxes_ewald(const float *px, const float *py, const float *pz,
+                                              const float *node_table, int32_t *workspace,
+                                              float *force, int64_t n, const uint64_t *codes,
+                                              int box_bits, const int32_t *box_roots,
+                                              const float *box_params,
+                                              const float *theta_per_bucket, int bodies_per_lane,
+                                              int block_warps, double G, const float *ewald_table,
+                                              int ewald_nt, unsigned long long *stats,
+                                              int32_t *status, void *stream) {
+    GroupedParams P;
+    CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket,
+                           CNB_MAC_REF_X, bodies_per_lane, block_warps, G, stats, status));
+    if (n == 0) return CNB_OK;
+    if (!codes || !box_roots || !box_params || box_bits < 0 || box_bits > 30)
+        return CNB_E_INVALID_ARG;
+    if (!ewald_table || ewald_nt < 2 || ewald_nt > 512 ||
+        (reinterpret_cast<uintptr_t>(ewald_table) & 15) ||
+        (reinterpret_cast<uintptr_t>(box_params) & 15))
+        return CNB_E_INVALID_ARG;
+    P.mac = CNB_MAC_EWALD;
+    P.codes = codes;
+    P.box_shift = 3 * ((63 - box_bits) / 3);
+    P.box_roots = box_roots;
+    P.box_params = reinterpret_cast<const float4 *>(box_params);
+    P.ewald = reinterpret_cast<const float4 *>(ewald_table);
+    P.ewald_nt = ewald_nt;
+    return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
+}
+
 extern "C" int cnb_forces_grouped_boxes(const float *px, const float *py, const float *pz,
                                         const float *node_table, int32_t *workspace, float *force,
                                         int64_t n, const uint64_t *codes, int box_bits,

@@ -290,6 +290,17 @@ int cnb_forces_grouped_ewald(const float *px, const float *py, const float *pz,
                              int ewald_nt, unsigned long long *stats, int32_t *status,
                              void *stream);
 
+/* cnb_forces_grouped_boxes under the periodic law of cnb_forces_grouped_ewald:
+ * every box is periodic on its own unit cube. */
+int cnb_forces_grouped_boxes_ewald(const float *px, const float *py, const float *pz,
+                                   const float *node_table, int32_t *workspace, float *force,
+                                   int64_t n, const uint64_t *codes, int box_bits,
+                                   const int32_t *box_roots, const float *box_params,
+                                   const float *theta_per_bucket, int bodies_per_lane,
+                                   int block_warps, double G, const float *ewald_table,
+                                   int ewald_nt, unsigned long long *stats, int32_t *status,
+                                   void *stream);
+
 /* Float64 periodic direct sum for the bodies listed in targets (accuracy
  * oracle of the periodic law): per pair the softened monopole at the minimum
  * image plus f_per - d/|d|^3, with the Ewald sums carried to float64
