@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--warps", type=int, default=8, choices=[2, 4, 8],
                     help="warps per block of the grouped traversal (with --no-tune)")
     ap.add_argument("--slab", type=float, default=0, help="periodic test: slab tolerance in bodies")
+    ap.add_argument("--quad", action="store_true",
+                    help="with --mac ewald: internal nodes also apply their quadrupole moments")
     ap.add_argument("--super", type=int, default=0,
                     help="super-bucket size of the two-level walk (ref_x test; 0 = single level)")
     ap.add_argument("--width", type=int, default=1920)
@@ -82,7 +84,7 @@ def make_config(args, seed):
                        FORCE_MODE=args.force_mode, MAC=args.mac, PRECISION=args.precision,
                        UPWARD=args.upward, RES=args.width, RES_W=args.width, RES_H=args.height,
                        SEED=seed, BODIES_PER_LANE=args.bpl, SLAB_BODIES=args.slab,
-                       SUPER_BODIES=args.super, BLOCK_WARPS=args.warps)
+                       SUPER_BODIES=args.super, BLOCK_WARPS=args.warps, QUADRUPOLE=args.quad)
 
 
 def dist_init():
@@ -283,7 +285,7 @@ def config_dict(cfg, args):
     return {"workload": f"Zel'dovich {cfg.N_GRID}^3 plain Barnes-Hut step + {cfg.RES_W}x{cfg.RES_H} splat",
             "n_bodies": cfg.N_BODIES, "theta": cfg.THETA, "softening": cfg.SOFTENING,
             "da": 0.002, "a_start": cfg.A_START, "seed": 1, "keys": "morton63",
-            "force_mode": cfg.FORCE_MODE, "mac": cfg.MAC, "upward": cfg.UPWARD,
+            "force_mode": cfg.FORCE_MODE, "mac": cfg.MAC, "quadrupole": cfg.QUADRUPOLE, "upward": cfg.UPWARD,
             "precision": cfg.PRECISION,
             "bodies_per_lane": cfg.BODIES_PER_LANE, "slab_bodies": cfg.SLAB_BODIES,
             "l2": "flushed between timed steps (256 MB write)", "parallelism": f"replicas x{args.gpus}"}

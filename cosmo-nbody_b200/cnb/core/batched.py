@@ -112,7 +112,7 @@ class BatchedBoxes:
         self.ewald_table = None
         if self.mac == _lib.MAC_EWALD:
             # every box is periodic on its own unit cube: one correction table serves all
-            self.ewald_table = z((EWALD_NT + 1) ** 3, 12)
+            self.ewald_table = z((EWALD_NT + 1) ** 3, 24)
             _lib.call("cnb_ewald_table", self.ewald_table.data_ptr(), EWALD_NT, self._st())
         self._ctx = SortContext(n)
         self._graph = None

@@ -42,10 +42,13 @@ class SimulationEngine:
             raise ValueError("FORCE_MODE must be 'reference' or 'grouped'")
         self.bodies_per_lane = int(getattr(config, "BODIES_PER_LANE", 1))
         self.block_warps = int(getattr(config, "BLOCK_WARPS", 8))
+        self.quadrupole = bool(getattr(config, "QUADRUPOLE", False))
+        if self.quadrupole and getattr(config, "MAC", "ref_x") != "ewald":
+            raise ValueError("QUADRUPOLE needs MAC 'ewald'")
         self.tree_manager = OctreeManager(state.n, config.TPB, device=state.device,
                                           upward=getattr(config, "UPWARD", "plain"),
                                           node_table=self.force_mode == "grouped",
-                                          bucket=32 * self.bodies_per_lane)
+                                          bucket=32 * self.bodies_per_lane, quad=self.quadrupole)
         res = getattr(config, "RES", 1024)
         self.camera = Camera(config.N_STEPS, res, config, device=state.device) if camera else None
         self.cache_size = getattr(config, "CACHE_SIZE", 256)
@@ -68,7 +71,7 @@ class SimulationEngine:
         if self.mac == _lib.MAC_EWALD:
             if self.force_mode != "grouped":
                 raise ValueError("MAC 'ewald' needs FORCE_MODE 'grouped'")
-            self.ewald_table = torch.empty(((EWALD_NT + 1) ** 3, 12), dtype=torch.float32,
+            self.ewald_table = torch.empty(((EWALD_NT + 1) ** 3, 24), dtype=torch.float32,
                                            device=state.device)
             _lib.call("cnb_ewald_table", self.ewald_table.data_ptr(), EWALD_NT, self._stream())
         self.super_bodies = 0
@@ -116,7 +119,9 @@ class SimulationEngine:
                           tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,
                           float(cfg.THETA), tpg.data_ptr() if tpg is not None else None,
                           self.bodies_per_lane, self.block_warps, float(cfg.G), float(cfg.SOFTENING),
-                          self.ewald_table.data_ptr(), EWALD_NT, self.stats.data_ptr(), status, st)
+                          self.ewald_table.data_ptr(), EWALD_NT,
+                          tm.quad.data_ptr() if tm.quad is not None else None,
+                          self.stats.data_ptr(), status, st)
                 return
             if self.super_ws is not None and tpg is None:
                 _lib.call("cnb_forces_two_level", px.data_ptr(), py.data_ptr(), pz.data_ptr(),

@@ -23,7 +23,7 @@ class OctreeManager:
     """octree.py:13-93."""
 
     def __init__(self, n_bodies, tpb=256, device=None, upward="plain", node_table=False,
-                 bucket=32):
+                 bucket=32, quad=False):
         self.n = int(n_bodies)
         self.n_nodes = max(2 * self.n - 1, 1)
         self.tpb = tpb
@@ -54,6 +54,10 @@ class OctreeManager:
             self.ranges = torch.zeros((max(self.n - 1, 1), 2), dtype=torch.int32, device=dev)
             self.workspace = torch.zeros(4 + 4 * max(self.n, 1), dtype=torch.int32, device=dev)
             self.bucket = int(bucket)
+        # second central moments of the internal nodes (grouped plain upward only)
+        self.quad = torch.zeros((m, 8), dtype=torch.float32, device=dev) if quad else None
+        if quad and (not node_table or upward != "plain"):
+            raise ValueError("quad needs node_table=True and the plain upward pass")
 
     def _stream(self):
         return int(torch.cuda.current_stream(self.device).cuda_stream)
@@ -73,10 +77,16 @@ class OctreeManager:
         px, py, pz = pos_d
         if self.node_table is not None and self.upward == "plain":
             # one pass: sums, boxes and the traversal table; com stays raw until asked for
-            _lib.call("cnb_upward_table", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
-                      mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
-                      self.counters.data_ptr(), self.node_table.data_ptr(), self.sums.data_ptr(),
-                      n, status, st)
+            if self.quad is not None:
+                _lib.call("cnb_upward_table_quad", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                          mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
+                          self.counters.data_ptr(), self.node_table.data_ptr(),
+                          self.sums.data_ptr(), self.quad.data_ptr(), n, status, st)
+            else:
+                _lib.call("cnb_upward_table", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                          mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
+                          self.counters.data_ptr(), self.node_table.data_ptr(), self.sums.data_ptr(),
+                          n, status, st)
             self._stale_ref = True
             _lib.call("cnb_find_root", self.parent.data_ptr(), self.root_idx.data_ptr(), m, st)
             _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), n,

@@ -3,6 +3,7 @@
     python -m cnb.studies precision   [--n-grid 256] [--steps 50]
     python -m cnb.studies batched     [--boxes 64] [--steps 10]
     python -m cnb.studies controller  [--n-grid 128] [--evolve 100] [--mac ewald]
+    python -m cnb.studies multipole   [--n-grid 128] [--evolve 100]
 
 precision:  Zel'dovich n^3 (seed 2) evolved `steps` kick-drift steps from
             a = 0.02 with da = 0.002; then, for theta in {0.3, 0.5, 0.7}, both
@@ -19,6 +20,9 @@ controller: labels from the batched boxes, training on the GPU, and learned
             on an evolved n^3 state (seed 4); under the minimum-image law with
             the exact periodic test (default), or with --mac ewald under the
             periodic (Ewald) law, each against its own float64 direct sum.
+multipole:  under the periodic law on the same evolved state: monopoles at
+            theta = 0.5 against quadrupoles over a theta grid (p99 error
+            against the float64 Ewald direct sum, interactions, forces ms).
 Each prints one JSON object per configuration.
 """
 from __future__ import annotations
@@ -258,9 +262,50 @@ def controller(args):
                           seconds=time.time() - t0)), flush=True)
 
 
+def multipole(args):
+    t0 = time.time()
+    pos, vel, a = _evolve(args.n_grid, 4, args.evolve)
+    n = args.n_grid ** 3
+    targets = np.sort(np.random.default_rng(0).choice(n, 1024, replace=False)).astype(np.int64)
+    ref = None
+    rows = []
+    for quad, thetas in ((False, (0.5,)), (True, (0.5, 0.6, 0.7, 0.8, 0.9, 1.0))):
+        cfg = _cfg(args.n_grid, MAC="ewald", QUADRUPOLE=quad, BODIES_PER_LANE=args.bpl, BLOCK_WARPS=4)
+        st = SimulationState(n, pos, vel)
+        eng = SimulationEngine(cfg, st, camera=False)
+        eng.forces_only()
+        if ref is None:
+            ref = _direct(st, targets, cfg.SOFTENING, periodic=True)
+        for th in thetas:
+            eng.config.THETA = th
+            eng.compute_forces()
+            best = float("inf")
+            for _ in range(3):
+                eng.stats.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                eng.compute_forces()
+                e1.record()
+                torch.cuda.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            s = eng.stats.cpu().numpy()
+            rows.append(dict(quadrupole=quad, theta=th, forces_ms=best, interactions=float(s[0]) / n,
+                             quadrupole_interactions=float(s[2]) / n if quad else 0.0,
+                             **_errors(st.force, ref, targets)))
+        eng.check()
+        del eng, st
+    base = rows[0]
+    ok = [r for r in rows[1:] if r["p99_rms"] <= base["p99_rms"]]
+    best = max(ok, key=lambda r: r["theta"]) if ok else None
+    print(json.dumps(dict(study="multipole", law="ewald", n_grid=args.n_grid, evolve_steps=args.evolve,
+                          a=a, rows=rows, monopole_theta05=base, quadrupole_at_equal_p99=best,
+                          speedup_forces=(base["forces_ms"] / best["forces_ms"]) if best else None,
+                          seconds=time.time() - t0)), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("study", choices=["precision", "batched", "controller"])
+    ap.add_argument("study", choices=["precision", "batched", "controller", "multipole"])
     ap.add_argument("--n-grid", type=int, default=None)
     ap.add_argument("--steps", type=int, default=None)
     ap.add_argument("--boxes", type=int, default=64)
@@ -278,6 +323,9 @@ def main():
     elif args.study == "batched":
         args.steps = args.steps or 10
         batched(args)
+    elif args.study == "multipole":
+        args.n_grid = args.n_grid or 128
+        multipole(args)
     else:
         args.n_grid = args.n_grid or 128
         controller(args)

@@ -44,6 +44,7 @@ PRECISION = "f32"          # per-particle traversal arithmetic: "f32" or "f64" (
 UPWARD = "plain"           # "plain": bit-exact upward pass; "compensated": two-sum + float64 root
 BODIES_PER_LANE = 1        # grouped traversal: bodies per lane (buckets of 32 x this)
 BLOCK_WARPS = 8            # grouped traversal: warps per block (2, 4 or 8)
+QUADRUPOLE = False         # "ewald" test: internal nodes also apply their quadrupole moments
 SUPER_BODIES = 0           # grouped "ref_x" traversal: super-bucket size of the two-level walk (0 = off)
 SLAB_BODIES = 0            # periodic test: image-ambiguous nodes up to this many bodies' mass are
                            # applied with the per-pair minimum image (0 = exact)

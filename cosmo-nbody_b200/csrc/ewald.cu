@@ -9,7 +9,8 @@
 // d_n = d - n, k = 2 pi m.  Near d = 0, f_per(d) = d / |d|^3 - (4 pi / 3) d
 // + g(d) with g smooth, odd and O(|d|^3).
 //
-// cnb_ewald_table tabulates g and its Jacobian on the octant [0, 1/2]^3 in
+// cnb_ewald_table tabulates g, its Jacobian and its second derivatives on
+// the octant [0, 1/2]^3 in
 // float64 arithmetic (stored as float32); the grouped traversal's "ewald"
 // test reads it.  cnb_direct_sum_ewald_f64 is the float64 accuracy oracle:
 // every pair's periodic force to float64 precision.
@@ -107,8 +108,12 @@ __device__ void ewald_force(const double d[3], bool without_mono, double f[3], d
         for (int q = 0; q < 6; ++q) jac[q] = J[q];
 }
 
-// Grid point (i, j, k) of the octant, spacing 1 / (2 nt): g and its
-// Jacobian, (gx, gy, gz, 0 | Jxx, Jxy, Jxz, Jyy | Jyz, Jzz, 0, 0).
+// Grid point (i, j, k) of the octant, spacing 1 / (2 nt): g, its Jacobian
+// and its second derivatives H_ijk = d^2 g_i / d_j d_k (symmetric in all
+// three indices, g being the gradient of a potential), six float4:
+//   (gx, gy, gz, 0 | Jxx, Jxy, Jxz, Jyy | Jyz, Jzz, 0, 0 |
+//    Hxxx, Hxxy, Hxxz, Hxyy | Hxyz, Hxzz, Hyyy, Hyyz | Hyzz, Hzzz, 0, 0).
+// H by central differences of the analytic Jacobian (step 1e-4, float64).
 __global__ void __launch_bounds__(128) k_ewald_table(float4 *table, int nt) {
     const int64_t pts = (int64_t)(nt + 1) * (nt + 1) * (nt + 1);
     const double h = 0.5 / nt;
@@ -121,12 +126,31 @@ __global__ void __launch_bounds__(128) k_ewald_table(float4 *table, int nt) {
         const double d[3] = {i * h, j * h, k * h};
         double f[3], J[6];
         ewald_force(d, true, f, J);
+        // dJ/dd_k: the diagonal (linear) term drops out of the differences
+        constexpr double kStep = 1e-4;
+        double dJ[3][6];
+        for (int k2 = 0; k2 < 3; ++k2) {
+            double dp[3] = {d[0], d[1], d[2]}, dm[3] = {d[0], d[1], d[2]};
+            dp[k2] += kStep;
+            dm[k2] -= kStep;
+            double fp[3], fm[3], Jp[6], Jm[6];
+            ewald_force(dp, true, fp, Jp);
+            ewald_force(dm, true, fm, Jm);
+            for (int q = 0; q < 6; ++q) dJ[k2][q] = (Jp[q] - Jm[q]) / (2.0 * kStep);
+        }
+        // J index: xx 0, xy 1, xz 2, yy 3, yz 4, zz 5; H_ijk = dJ_ij / dd_k
+        const double Hxxx = dJ[0][0], Hxxy = dJ[1][0], Hxxz = dJ[2][0], Hxyy = dJ[1][1];
+        const double Hxyz = dJ[2][1], Hxzz = dJ[2][2], Hyyy = dJ[1][3], Hyyz = dJ[2][3];
+        const double Hyzz = dJ[2][4], Hzzz = dJ[2][5];
+        float4 *row = table + 6 * t;
         // g = f_per - mono + (4 pi / 3) d; its Jacobian gains (4 pi / 3) I
-        table[3 * t] = make_float4((float)(f[0] + lin * d[0]), (float)(f[1] + lin * d[1]),
-                                   (float)(f[2] + lin * d[2]), 0.f);
-        table[3 * t + 1] = make_float4((float)(J[0] + lin), (float)J[1], (float)J[2],
-                                       (float)(J[3] + lin));
-        table[3 * t + 2] = make_float4((float)J[4], (float)(J[5] + lin), 0.f, 0.f);
+        row[0] = make_float4((float)(f[0] + lin * d[0]), (float)(f[1] + lin * d[1]),
+                             (float)(f[2] + lin * d[2]), 0.f);
+        row[1] = make_float4((float)(J[0] + lin), (float)J[1], (float)J[2], (float)(J[3] + lin));
+        row[2] = make_float4((float)J[4], (float)(J[5] + lin), 0.f, 0.f);
+        row[3] = make_float4((float)Hxxx, (float)Hxxy, (float)Hxxz, (float)Hxyy);
+        row[4] = make_float4((float)Hxyz, (float)Hxzz, (float)Hyyy, (float)Hyyz);
+        row[5] = make_float4((float)Hyzz, (float)Hzzz, 0.f, 0.f);
     }
 }
 

@@ -70,6 +70,9 @@ struct GroupedParams {
     // CNB_MAC_EWALD: g and its Jacobian on the octant grid (cnb_ewald_table)
     const float4 *ewald;
     int ewald_nt;
+    // CNB_MAC_EWALD: second central moments of internal nodes (two float4 per
+    // node, cnb_upward_table_quad), null = monopoles only
+    const float4 *quad;
 };
 
 // Periodic correction of one accepted node, d = its CoM image minus the
@@ -83,7 +86,7 @@ __device__ __forceinline__ void ewald_lookup(const float4 *__restrict__ T, int n
     const int i = min(__float2int_rn(ax * sc), nt), j = min(__float2int_rn(ay * sc), nt),
               k = min(__float2int_rn(az * sc), nt);
     const int64_t t = ((int64_t)i * (nt + 1) + j) * (nt + 1) + k;
-    const float4 t0 = __ldg(T + 3 * t), t1 = __ldg(T + 3 * t + 1), t2 = __ldg(T + 3 * t + 2);
+    const float4 t0 = __ldg(T + 6 * t), t1 = __ldg(T + 6 * t + 1), t2 = __ldg(T + 6 * t + 2);
     const float h = 1.f / sc;
     const float ex = ax - i * h, ey = ay - j * h, ez = az - k * h;
     // octant: g(a) = g(a0) + J(a0) (a - a0); J = (xx, xy, xz, yy, yz, zz)
@@ -100,6 +103,28 @@ __device__ __forceinline__ void ewald_lookup(const float4 *__restrict__ T, int n
     J[3] = t1.w;
     J[4] = sy * sz * t2.x;
     J[5] = t2.y;
+}
+
+// The periodic part of a node's quadrupole force, (1/2) H(d) : M2, with H
+// (the second derivatives of g) at the table point nearest d and M2 the
+// node's second central moment (xx, xy, xz, yy | yz, zz).
+__device__ __forceinline__ void ewald_quad(const float4 *__restrict__ T, int nt, float dx, float dy,
+                                           float dz, float4 ma, float4 mb, float (&out)[3]) {
+    const float sc = 2.f * nt;
+    const int i = min(__float2int_rn(fabsf(dx) * sc), nt), j = min(__float2int_rn(fabsf(dy) * sc), nt),
+              k = min(__float2int_rn(fabsf(dz) * sc), nt);
+    const int64_t t = ((int64_t)i * (nt + 1) + j) * (nt + 1) + k;
+    const float4 h0 = __ldg(T + 6 * t + 3), h1 = __ldg(T + 6 * t + 4), h2 = __ldg(T + 6 * t + 5);
+    const float sx = dx < 0.f ? -1.f : 1.f, sy = dy < 0.f ? -1.f : 1.f, sz = dz < 0.f ? -1.f : 1.f;
+    // H_ijk(d) = s_i s_j s_k H_ijk(|d|)
+    const float xxx = sx * h0.x, xxy = sy * h0.y, xxz = sz * h0.z, xyy = sx * h0.w;
+    const float xyz = sx * sy * sz * h1.x, xzz = sx * h1.y, yyy = sy * h1.z, yyz = sz * h1.w;
+    const float yzz = sy * h2.x, zzz = sz * h2.y;
+    const float mxx = ma.x, mxy = ma.y, mxz = ma.z, myy = ma.w, myz = mb.x, mzz = mb.y;
+    // (1/2) sum_jk H_ijk M_jk, off-diagonal pairs counted twice
+    out[0] = 0.5f * (xxx * mxx + xyy * myy + xzz * mzz) + xxy * mxy + xxz * mxz + xyz * myz;
+    out[1] = 0.5f * (xxy * mxx + yyy * myy + yzz * mzz) + xyy * mxy + xyz * mxz + yyz * myz;
+    out[2] = 0.5f * (xxz * mxx + yyz * myy + zzz * mzz) + xyz * mxy + xzz * mxz + yzz * myz;
 }
 
 // Nearest-image offset of a coordinate difference d with |d| < 1.5:
@@ -246,10 +271,85 @@ __device__ __forceinline__ void apply_entries(const float4 *list, int cnt, const
         apply_list<BPL, WRAP>(list, cnt, x, y, z, soft2, ax, ay, az);
 }
 
-template <int BPL>
+// float4 slots per entry of the second list: the per-pair-image list, or
+// under the periodic law the quadrupole list (position and mass | xx, xy, xz,
+// yy | yz, zz, trace, 0 of the node's second central moment)
+template <int BPL, bool EWALD> __host__ __device__ constexpr int second_width() {
+    return EWALD ? 3 : entry_width<BPL>();
+}
+
+template <int BPL, bool EWALD>
 constexpr size_t grouped_smem(int warps) {
     return (size_t)warps * (kGStack * sizeof(int32_t) +
-                            2 * kGList * entry_width<BPL>() * sizeof(float4));
+                            kGList * (entry_width<BPL>() + second_width<BPL, EWALD>()) *
+                                sizeof(float4));
+}
+
+// Applies cnt quadrupole entries: per body the softened monopole plus
+// (15/2)(d.M d) d / r^7 - 3 M d / r^5 - (3/2) tr(M) d / r^5 for the node's
+// second central moment M about its CoM (d = CoM - body, r softened).
+template <int BPL>
+__device__ __forceinline__ void apply_quad(const float4 *q, int cnt, const float (&x)[BPL],
+                                           const float (&y)[BPL], const float (&z)[BPL],
+                                           float soft2, float (&ax)[BPL], float (&ay)[BPL],
+                                           float (&az)[BPL]) {
+    const float cut = soft2 + 1e-7f;
+    if constexpr (BPL == 2) {
+        // two bodies per lane as packed float2 (FADD2 / FMUL2 / FFMA2)
+        const float2 nx = make_float2(-x[0], -x[1]), ny = make_float2(-y[0], -y[1]),
+                     nz = make_float2(-z[0], -z[1]);
+        const float2 s2 = make_float2(soft2, soft2);
+        float2 fx = make_float2(ax[0], ax[1]), fy = make_float2(ay[0], ay[1]),
+               fz = make_float2(az[0], az[1]);
+        const auto dup = [](float a) { return make_float2(a, a); };
+#pragma unroll 2
+        for (int j = 0; j < cnt; ++j) {
+            const float4 e = q[3 * j], u = q[3 * j + 1], v = q[3 * j + 2];
+            const float2 dx = __fadd2_rn(dup(e.x), nx), dy = __fadd2_rn(dup(e.y), ny),
+                         dz = __fadd2_rn(dup(e.z), nz);
+            const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
+            const float2 ri = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+            const float2 ri2 = __fmul2_rn(ri, ri), ri3 = __fmul2_rn(ri2, ri);
+            const float2 ri5 = __fmul2_rn(ri3, ri2), ri7 = __fmul2_rn(ri5, ri2);
+            const float2 qx = __ffma2_rn(dup(u.x), dx, __ffma2_rn(dup(u.y), dy, __fmul2_rn(dup(u.z), dz)));
+            const float2 qy = __ffma2_rn(dup(u.y), dx, __ffma2_rn(dup(u.w), dy, __fmul2_rn(dup(v.x), dz)));
+            const float2 qz = __ffma2_rn(dup(u.z), dx, __ffma2_rn(dup(v.x), dy, __fmul2_rn(dup(v.y), dz)));
+            const float2 sq = __ffma2_rn(dx, qx, __ffma2_rn(dy, qy, __fmul2_rn(dz, qz)));
+            float2 A = __ffma2_rn(dup(e.w), ri3,
+                                  __ffma2_rn(__fmul2_rn(dup(7.5f), sq), ri7, __fmul2_rn(dup(-1.5f * v.z), ri5)));
+            float2 B = __fmul2_rn(dup(-3.f), ri5);
+            if (!(r2.x > cut)) A.x = B.x = 0.f;
+            if (!(r2.y > cut)) A.y = B.y = 0.f;
+            fx = __ffma2_rn(A, dx, __ffma2_rn(B, qx, fx));
+            fy = __ffma2_rn(A, dy, __ffma2_rn(B, qy, fy));
+            fz = __ffma2_rn(A, dz, __ffma2_rn(B, qz, fz));
+        }
+        ax[0] = fx.x; ax[1] = fx.y;
+        ay[0] = fy.x; ay[1] = fy.y;
+        az[0] = fz.x; az[1] = fz.y;
+        return;
+    }
+#pragma unroll 2
+    for (int j = 0; j < cnt; ++j) {
+        const float4 e = q[3 * j], u = q[3 * j + 1], v = q[3 * j + 2];
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) {
+            const float dx = e.x - x[b], dy = e.y - y[b], dz = e.z - z[b];
+            const float r2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
+            const float ri = rsqrtf(r2);
+            const float ri2 = ri * ri, ri3 = ri2 * ri, ri5 = ri3 * ri2, ri7 = ri5 * ri2;
+            const float qx = fmaf(u.x, dx, fmaf(u.y, dy, u.z * dz));
+            const float qy = fmaf(u.y, dx, fmaf(u.w, dy, v.x * dz));
+            const float qz = fmaf(u.z, dx, fmaf(v.x, dy, v.y * dz));
+            const float sq = fmaf(dx, qx, fmaf(dy, qy, dz * qz));
+            float A = fmaf(e.w, ri3, fmaf(7.5f * sq, ri7, -1.5f * v.z * ri5));
+            float B = -3.f * ri5;
+            if (!(r2 > cut)) A = B = 0.f;
+            ax[b] = fmaf(A, dx, fmaf(B, qx, ax[b]));
+            ay[b] = fmaf(A, dy, fmaf(B, qy, ay[b]));
+            az[b] = fmaf(A, dz, fmaf(B, qz, az[b]));
+        }
+    }
 }
 
 template <int BPL, int WARPS, bool EWALD>
@@ -258,12 +358,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
     // two interaction lists per warp: entries with one image for the whole
-    // bucket, and entries needing the per-pair image
+    // bucket, and entries needing the per-pair image (under the periodic law:
+    // internal nodes with their quadrupole moments)
     constexpr int EW = entry_width<BPL>();
-    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * 2 * kGList * EW;
+    constexpr int SW = second_width<BPL, EWALD>();
+    float4 *list = reinterpret_cast<float4 *>(g_smem) + wib * kGList * (EW + SW);
     float4 *wlist = list + kGList * EW;
     int32_t *stack =
-        reinterpret_cast<int32_t *>(g_smem + WARPS * 2 * kGList * EW * sizeof(float4)) +
+        reinterpret_cast<int32_t *>(g_smem + WARPS * kGList * (EW + SW) * sizeof(float4)) +
         wib * kGStack;
     unsigned long long n_tests = 0;
     int max_top = 0;
@@ -403,7 +505,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                         const float tz = fmaxf(fabsf(dz) - ghz, 0.f);
                         const float d2min = tx * tx + ty * ty + tz * tz;
                         if (EWALD) {
-                            // periodic law: every image is valid, the 3-D extent decides
+                            // periodic law: every image is valid; the node's size is its
+                            // 3-D extent, or b_max when quadrupoles are applied
                             accept = S.y * S.y < th2 * d2min;
                         } else if (P.mac == CNB_MAC_REF_X) {
                             const float s = S.x > half_box ? P.box : S.x;
@@ -445,14 +548,30 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             n_tests += (node >= 0);
             const uint32_t am = __ballot_sync(0xffffffffu, accept);
             const uint32_t om = __ballot_sync(0xffffffffu, open);
-            const bool to_w = accept && E.w < 0.f;
+            // second list: per-pair image, or (periodic law) an internal node's quadrupole
+            const bool to_w = EWALD ? (accept && P.quad != nullptr && c0 != -1) : (accept && E.w < 0.f);
             const uint32_t wm = __ballot_sync(0xffffffffu, to_w);
             const uint32_t nm = am & ~wm;
             if (accept) {
-                if (to_w)
-                    put_entry<BPL>(wlist, wcnt + __popc(wm & lt), make_float4(E.x, E.y, E.z, -E.w));
-                else
+                if (to_w) {
+                    const int w = wcnt + __popc(wm & lt);
+                    if (EWALD) {
+                        const float4 qa = __ldg(P.quad + 2 * node), qb = __ldg(P.quad + 2 * node + 1);
+                        wlist[3 * w] = E;
+                        wlist[3 * w + 1] = qa;
+                        wlist[3 * w + 2] = make_float4(qb.x, qb.y, qa.x + qa.w + qb.y, 0.f);
+                        // and the periodic part of its quadrupole, a bucket constant
+                        float pq[3];
+                        ewald_quad(P.ewald, P.ewald_nt, E.x - gcx, E.y - gcy, E.z - gcz, qa, qb, pq);
+                        eg[0] += pq[0];
+                        eg[1] += pq[1];
+                        eg[2] += pq[2];
+                    } else {
+                        put_entry<BPL>(wlist, w, make_float4(E.x, E.y, E.z, -E.w));
+                    }
+                } else {
                     put_entry<BPL>(list, cnt + __popc(nm & lt), E);
+                }
             }
             cnt += __popc(nm);
             wcnt += __popc(wm);
@@ -480,19 +599,25 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                 __syncwarp();
             }
             if (wcnt >= 32) {
-                apply_entries<BPL, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
+                if (EWALD)
+                    apply_quad<BPL>(wlist, 32, x, y, z, soft2, ax, ay, az);
+                else
+                    apply_entries<BPL, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 n_wrap += 32;
                 __syncwarp();
 #pragma unroll
-                for (int w = 0; w < EW; ++w)
-                    if (lane < wcnt - 32) wlist[EW * lane + w] = wlist[EW * (32 + lane) + w];
+                for (int w = 0; w < SW; ++w)
+                    if (lane < wcnt - 32) wlist[SW * lane + w] = wlist[SW * (32 + lane) + w];
                 wcnt -= 32;
                 __syncwarp();
             }
         }
         apply_entries<BPL, false>(list, cnt, x, y, z, soft2, ax, ay, az);
-        apply_entries<BPL, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
+        if (EWALD)
+            apply_quad<BPL>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
+        else
+            apply_entries<BPL, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
         n_entries += cnt + wcnt;
         n_wrap += wcnt;
         __syncwarp();
@@ -740,7 +865,7 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
 
 template <int BPL, int WARPS, bool EWALD>
 static int launch_shape(GroupedParams &P, cudaStream_t st) {
-    const size_t smem = grouped_smem<BPL>(WARPS);
+    const size_t smem = grouped_smem<BPL, EWALD>(WARPS);
     CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS, EWALD>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
@@ -913,7 +1038,8 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
                                         int64_t n, double theta, const float *theta_per_bucket,
                                         int bodies_per_lane, int block_warps, double G, double soft,
                                         const float *ewald_table, int ewald_nt,
-                                        unsigned long long *stats, int32_t *status, void *stream) {
+                                        const float *quad, unsigned long long *stats,
+                                        int32_t *status, void *stream) {
     GroupedParams P;
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket,
                            CNB_MAC_REF_X, bodies_per_lane, block_warps, G, stats, status));
@@ -927,6 +1053,8 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
     P.box = 1.0f;
     P.ewald = reinterpret_cast<const float4 *>(ewald_table);
     P.ewald_nt = ewald_nt;
+    if (quad && (reinterpret_cast<uintptr_t>(quad) & 15)) return CNB_E_INVALID_ARG;
+    P.quad = reinterpret_cast<const float4 *>(quad);
     return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }
 

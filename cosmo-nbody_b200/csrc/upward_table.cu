@@ -38,11 +38,35 @@ __device__ __forceinline__ void store_record(float4 *rec, float4 *aabb, int64_t 
     aabb[2 * v + 1] = hi;
 }
 
+// Second central moment of the union of two children (parallel-axis rule):
+// M2 = M2_l + m_l (c_l - c)(c_l - c)^T + M2_r + m_r (c_r - c)(c_r - c)^T,
+// six components (xx, xy, xz, yy, yz, zz) in two float4s.
+__device__ __forceinline__ void moment_add(float4 &a, float4 &b, float m, float dx, float dy,
+                                           float dz) {
+    a.x = fmaf(m * dx, dx, a.x);
+    a.y = fmaf(m * dx, dy, a.y);
+    a.z = fmaf(m * dx, dz, a.z);
+    a.w = fmaf(m * dy, dy, a.w);
+    b.x = fmaf(m * dy, dz, b.x);
+    b.y = fmaf(m * dz, dz, b.y);
+}
+
+__device__ __forceinline__ float3 centre_of(float4 s) {
+    const float inv = s.w > 0.f ? 1.f / s.w : 0.f;
+    return make_float3(s.x * inv, s.y * inv, s.z * inv);
+}
+
+// QUAD: also the second central moment of every internal node, quad[2v],
+// quad[2v + 1] (leaves hold none: a leaf's moment is zero and is never read),
+// and in the record's 3-D-extent slot the node's b_max instead: the largest
+// distance from its CoM to a corner of its box (no member lies farther), the
+// size the periodic-law opening test needs once quadrupoles are applied.
+template <bool QUAD>
 __global__ void __launch_bounds__(256) k_upward_table(
     const float *__restrict__ px, const float *__restrict__ py, const float *__restrict__ pz,
     const float *__restrict__ mass, const int2 *__restrict__ children,
     const int32_t *__restrict__ parents, int32_t *counts, float4 *sums, float4 *rec, float4 *aabb,
-    int64_t n, int32_t *status) {
+    float4 *quad, int64_t n, int32_t *status) {
     const int64_t m_nodes = 2 * n - 1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -50,6 +74,7 @@ __global__ void __launch_bounds__(256) k_upward_table(
         // tree_kernels.py:152-159 leaf: com = p * m (float32), box = p
         float4 s = make_float4(__fmul_rn(x, m), __fmul_rn(y, m), __fmul_rn(z, m), m);
         float4 lo = make_float4(x, y, z, 0.f), hi = lo;
+        float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;  // this node's moment (QUAD)
         sums[i] = s;
         store_record(rec, aabb, i, s, lo, hi, -1, -1);
         int64_t curr = i;
@@ -90,6 +115,26 @@ __global__ void __launch_bounds__(256) k_upward_table(
                                            umax(Lhi.z, Rhi.z), 0.f);
             sums[p] = qs;
             store_record(rec, aabb, p, qs, qlo, qhi, ch.x, ch.y);
+            if (QUAD) {
+                float4 ba = make_float4(0.f, 0.f, 0.f, 0.f), bb = ba;
+                if (sib >= n) {
+                    ba = __ldcg(quad + 2 * sib);
+                    bb = __ldcg(quad + 2 * sib + 1);
+                }
+                const float3 cp = centre_of(qs), cm = centre_of(s), cs = centre_of(bs);
+                float4 na = make_float4(qa.x + ba.x, qa.y + ba.y, qa.z + ba.z, qa.w + ba.w);
+                float4 nb = make_float4(qb.x + bb.x, qb.y + bb.y, 0.f, 0.f);
+                moment_add(na, nb, s.w, cm.x - cp.x, cm.y - cp.y, cm.z - cp.z);
+                moment_add(na, nb, bs.w, cs.x - cp.x, cs.y - cp.y, cs.z - cp.z);
+                quad[2 * p] = na;
+                quad[2 * p + 1] = nb;
+                const float bx = fmaxf(cp.x - qlo.x, qhi.x - cp.x);
+                const float by = fmaxf(cp.y - qlo.y, qhi.y - cp.y);
+                const float bz = fmaxf(cp.z - qlo.z, qhi.z - cp.z);
+                rec[2 * p + 1].y = sqrtf(fmaf(bx, bx, fmaf(by, by, bz * bz)));
+                qa = na;
+                qb = nb;
+            }
             s = qs;
             lo = qlo;
             hi = qhi;
@@ -141,9 +186,32 @@ extern "C" int cnb_upward_table(const float *px, const float *py, const float *p
     if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
     const int64_t m = 2 * n - 1;
     float4 *rec = reinterpret_cast<float4 *>(node_table);
-    k_upward_table<<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
+    k_upward_table<false><<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
         px, py, pz, mass, reinterpret_cast<const int2 *>(children), parents, counts,
-        reinterpret_cast<float4 *>(sums), rec, rec + 2 * m, n, status);
+        reinterpret_cast<float4 *>(sums), rec, rec + 2 * m, nullptr, n, status);
+    return launch_status();
+}
+
+extern "C" int cnb_upward_table_quad(const float *px, const float *py, const float *pz,
+                                     const float *mass, const int32_t *children,
+                                     const int32_t *parents, int32_t *counts, float *node_table,
+                                     float *sums, float *quad, int64_t n, int32_t *status,
+                                     void *stream) {
+    if (n < 0) return CNB_E_INVALID_ARG;
+    if (n == 0) return CNB_OK;
+    if (!px || !py || !pz || !mass || !children || !parents || !counts || !node_table || !sums ||
+        !quad)
+        return CNB_E_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(node_table) & 15) || (reinterpret_cast<uintptr_t>(sums) & 15) ||
+        (reinterpret_cast<uintptr_t>(quad) & 15) || (reinterpret_cast<uintptr_t>(children) & 7))
+        return CNB_E_INVALID_ARG;
+    if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
+    const int64_t m = 2 * n - 1;
+    float4 *rec = reinterpret_cast<float4 *>(node_table);
+    k_upward_table<true><<<grid_for(n, 256), 256, 0, as_stream(stream)>>>(
+        px, py, pz, mass, reinterpret_cast<const int2 *>(children), parents, counts,
+        reinterpret_cast<float4 *>(sums), rec, rec + 2 * m, reinterpret_cast<float4 *>(quad), n,
+        status);
     return launch_status();
 }
 

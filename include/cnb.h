@@ -273,22 +273,39 @@ int cnb_forces_two_level(const float *px, const float *py, const float *pz,
  * all its images (neutralising background) is f_per(d) = d/|d|^3 -
  * (4 pi/3) d + g(d), g smooth and O(|d|^3).
  *
- * Tabulates g and its Jacobian on the octant [0, 1/2]^3, (nt + 1)^3 points
- * of spacing 1/(2 nt), computed in float64: table is float32
- * [(nt + 1)^3, 12] (16-byte aligned), 2 <= nt <= 512. */
+ * Tabulates g, its Jacobian and its second derivatives on the octant
+ * [0, 1/2]^3, (nt + 1)^3 points of spacing 1/(2 nt), computed in float64:
+ * table is float32 [(nt + 1)^3, 24] (16-byte aligned), 2 <= nt <= 512. */
 int cnb_ewald_table(float *table, int nt, void *stream);
 
 /* cnb_forces_grouped under the periodic law: nodes open on their 3-D extent
  * (l^2 < theta^2 dmin^2), one image of every accepted node serves the whole
  * bucket, each body gets the softened monopoles plus, for every accepted
  * node, -(4 pi/3) m (c - x) + m g(c - centre) + m J(c - centre) (centre - x)
- * with g, J from the table of cnb_ewald_table. */
+ * with g, J from the table of cnb_ewald_table.  quad (may be NULL): the
+ * second central moments of cnb_upward_table_quad; accepted internal nodes
+ * then also apply their quadrupole term, (15/2)(d.M d) d/r^7 - 3 M d/r^5 -
+ * (3/2) tr(M) d/r^5, plus its periodic part (1/2) H(c - centre) : M from
+ * the table's second derivatives of g (stats[2] then counts those
+ * quadrupole interactions). */
 int cnb_forces_grouped_ewald(const float *px, const float *py, const float *pz,
                              const float *node_table, int32_t *workspace, float *force, int64_t n,
                              double theta, const float *theta_per_bucket, int bodies_per_lane,
                              int block_warps, double G, double soft, const float *ewald_table,
-                             int ewald_nt, unsigned long long *stats, int32_t *status,
-                             void *stream);
+                             int ewald_nt, const float *quad, unsigned long long *stats,
+                             int32_t *status, void *stream);
+
+/* cnb_upward_table that also forms the second central moment of every
+ * internal node about its CoM (parallel-axis rule over the two children):
+ * quad is float32 [2 * n_nodes, 4] (16-byte aligned), node v at rows 2v,
+ * 2v+1: (xx, xy, xz, yy), (yz, zz, 0, 0); leaf rows are not written.  The
+ * node table's 3-D-extent slot then holds b_max, the largest distance from
+ * the node's CoM to a corner of its box, which the periodic-law opening test
+ * uses as the node's size. */
+int cnb_upward_table_quad(const float *px, const float *py, const float *pz, const float *mass,
+                          const int32_t *children, const int32_t *parents, int32_t *counts,
+                          float *node_table, float *sums, float *quad, int64_t n,
+                          int32_t *status, void *stream);
 
 /* cnb_forces_grouped_boxes under the periodic law of cnb_forces_grouped_ewald:
  * every box is periodic on its own unit cube. */

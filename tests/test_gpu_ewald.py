@@ -27,7 +27,7 @@ def _stream():
 
 def _table(nt):
     from cnb import _lib
-    t = torch.empty(((nt + 1) ** 3, 12), dtype=torch.float32, device="cuda")
+    t = torch.empty(((nt + 1) ** 3, 24), dtype=torch.float32, device="cuda")
     _lib.call("cnb_ewald_table", t.data_ptr(), nt, _stream())
     torch.cuda.synchronize()
     return t
@@ -58,6 +58,20 @@ def test_table_matches_float64_restatement():
     want = np.stack([J[:, 0, 0], J[:, 0, 1], J[:, 0, 2], J[:, 1, 1], J[:, 1, 2], J[:, 2, 2]], 1)
     got = np.concatenate([t[:, 4:8], t[:, 8:10]], 1)
     np.testing.assert_allclose(got, want, rtol=1e-5, atol=2e-5)
+    # second derivatives H_ijk = d J_ij / d d_k (xxx, xxy, xxz, xyy, xyz, xzz, yyy, yyz, yzz, zzz)
+    sel = np.nonzero(nz)[0][::7]
+    H = np.zeros((len(sel), 3, 3, 3))
+    hstep = 1e-3
+    for k in range(3):
+        e = np.zeros(3)
+        e[k] = hstep
+        H[:, :, :, k] = (_jac(d[sel] + e) - _jac(d[sel] - e)) / (2 * hstep)
+    idx = [(0, 0, 0), (0, 0, 1), (0, 0, 2), (0, 1, 1), (0, 1, 2), (0, 2, 2), (1, 1, 1), (1, 1, 2),
+           (1, 2, 2), (2, 2, 2)]
+    want_h = np.stack([H[:, i, j, k] for i, j, k in idx], 1)
+    got_h = np.concatenate([t[sel, 12:16], t[sel, 16:20], t[sel, 20:22]], 1)
+    np.testing.assert_allclose(got_h, want_h, rtol=1e-3, atol=2e-3)
+    assert np.abs(t[:, 22:24]).max() == 0.0
 
 
 def test_direct_sum_kernel_matches_restatement():
@@ -103,7 +117,8 @@ class Tree:
         status = torch.zeros(1, dtype=torch.int32, device="cuda")
         _lib.call("cnb_forces_grouped_ewald", *(p.data_ptr() for p in self.P),
                   self.tm.node_table.data_ptr(), self.tm.workspace.data_ptr(), f.data_ptr(), self.n,
-                  theta, None, self.bpl, 4, 1.0, soft, self.table.data_ptr(), 64, stats.data_ptr(),
+                  theta, None, self.bpl, 4, 1.0, soft, self.table.data_ptr(), 64,
+                  self.tm.quad.data_ptr() if self.tm.quad is not None else None, stats.data_ptr(),
                   status.data_ptr(), _stream())
         torch.cuda.synchronize()
         assert int(status.item()) == 0
@@ -269,3 +284,75 @@ def test_batched_boxes_follow_the_periodic_law_per_box():
         rms = np.sqrt(np.mean(np.sum(fe ** 2, 1)))
         assert np.median(diff) < 1e-3 * rms and np.percentile(diff, 99) < 0.05 * rms, \
             (np.median(diff) / rms, np.percentile(diff, 99) / rms)
+
+
+def test_upward_second_moments_match_direct_sums():
+    """cnb_upward_table_quad: every internal node's second central moment
+    equals the one summed directly over its bodies (a node of a Karras tree
+    covers a contiguous range of the sorted bodies); the traversal table is
+    the one the monopole pass writes."""
+    from cnb import _lib
+    from cnb.core.octree import OctreeManager
+    pos, codes = _sorted_bodies(16, 3)
+    n = codes.size
+    P = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in pos]
+    M = torch.full((n,), 1.0 / n, device="cuda")
+    K = torch.from_numpy(codes).cuda()
+    tq = OctreeManager(n, node_table=True, quad=True)
+    tq.build(P, M, K)
+    t0 = OctreeManager(n, node_table=True)
+    t0.build(P, M, K)
+    torch.cuda.synchronize()
+    # the same table, except that internal nodes carry b_max in the 3-D-extent slot
+    a_, b_ = tq.node_table.cpu().numpy(), t0.node_table.cpu().numpy()
+    rec_q, rec_0 = a_[0:2].reshape(-1, 2, 4), b_[0:2].reshape(-1, 2, 4)
+    np.testing.assert_array_equal(a_[2:], b_[2:])
+    np.testing.assert_array_equal(rec_q[:, 0], rec_0[:, 0])
+    np.testing.assert_array_equal(rec_q[:, 1, [0, 2, 3]], rec_0[:, 1, [0, 2, 3]])
+    np.testing.assert_array_equal(rec_q[:n, 1, 1], rec_0[:n, 1, 1])
+    q = tq.quad.cpu().numpy().astype(np.float64)
+    rg = tq.ranges.cpu().numpy()
+    p = np.stack(pos, 1).astype(np.float64)
+    rng = np.random.default_rng(0)
+    for i in rng.choice(n - 1, 400, replace=False):
+        lo, hi = int(rg[i, 0]), int(rg[i, 1])
+        b = p[lo:hi + 1]
+        m = 1.0 / n
+        c = b.mean(0)
+        s = b - c
+        M2 = m * s.T @ s
+        want = np.array([M2[0, 0], M2[0, 1], M2[0, 2], M2[1, 1], M2[1, 2], M2[2, 2]])
+        got = np.concatenate([q[n + i, 0:4], q[n + i, 4:6]])
+        scale = m * (hi - lo + 1) * np.max(np.sum(s * s, 1))
+        np.testing.assert_allclose(got, want, rtol=0, atol=2e-5 * scale + 1e-30)
+        # b_max bounds every member's distance from the CoM
+        bmax = float(rec_q[n + i, 1, 1])
+        assert np.sqrt(np.max(np.sum(s * s, 1))) <= bmax * (1 + 1e-5) + 1e-7
+
+
+def test_quadrupoles_lower_the_error():
+    from cnb.core.octree import OctreeManager
+    pos, codes = _sorted_bodies(32, 6)
+    soft = 0.5 / 32
+    tm = Tree(pos, codes)
+    f_mono, s_mono = tm.forces(0.5, soft)
+    tq = Tree.__new__(Tree)
+    tq.__dict__.update(tm.__dict__)
+    tq.tm = OctreeManager(tm.n, node_table=True, bucket=64, quad=True)
+    tq.tm.build(tm.P, tm.M, torch.from_numpy(codes).cuda())
+    f_quad, s_quad = tq.forces(0.5, soft)
+    # quadrupole mode opens on b_max (<= the 3-D extent's diagonal): fewer interactions
+    assert int(s_quad[2]) > 0
+    t = np.random.default_rng(1).choice(tm.n, 256, replace=False)
+    ref = tm.oracle(t, soft)
+    mm, pm = _errors(f_mono[t], ref)
+    mq, pq = _errors(f_quad[t], ref)
+    print(f"theta 0.5 monopole: median {mm:.2e} p99 {pm:.2e} ({s_mono[0] / tm.n:.0f}/body); "
+          f"quadrupole: median {mq:.2e} p99 {pq:.2e} ({s_quad[0] / tm.n:.0f}/body)")
+    # at the same theta: no worse than monopoles, with far fewer interactions
+    assert mq < mm and pq < pm and s_quad[0] < 0.7 * s_mono[0], (mm, mq, pm, pq)
+    # theta = 0 accepts leaves only: no quadrupole entries, the same forces
+    f0, s0 = tq.forces(0.0, soft)
+    g0, _ = tm.forces(0.0, soft)
+    assert int(s0[2]) == 0
+    np.testing.assert_array_equal(f0, g0)
