@@ -95,6 +95,7 @@ SIGNATURES = {
     "cnb_forces_grouped_ewald": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _d, _d, _p,
                                         _int, _p, _p, _p, _p]),
     "cnb_upward_table_quad": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
+    "cnb_upward_table_buckets": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_direct_sum_ewald_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_forces_grouped_boxes_ewald": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p, _int, _p, _p, _p, _int,
                                               _int, _d, _p, _int, _p, _p, _p]),

@@ -75,6 +75,19 @@ class OctreeManager:
         else:
             _lib.call("cnb_build_tree", codes_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(), n, st)
         px, py, pz = pos_d
+        if self.node_table is not None and self.upward == "plain" and self.bucket <= 64:
+            # buckets first (ranges and parents suffice), then sums, boxes and the
+            # traversal table bucket by bucket and above the buckets; com stays raw
+            _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), n,
+                      self.bucket, self.workspace.data_ptr(), st)
+            _lib.call("cnb_upward_table_buckets", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                      mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
+                      self.workspace.data_ptr(), self.counters.data_ptr(),
+                      self.node_table.data_ptr(), self.sums.data_ptr(),
+                      self.quad.data_ptr() if self.quad is not None else None, n, status, st)
+            self._stale_ref = True
+            _lib.call("cnb_find_root", self.parent.data_ptr(), self.root_idx.data_ptr(), m, st)
+            return self.root_idx
         if self.node_table is not None and self.upward == "plain":
             # one pass: sums, boxes and the traversal table; com stays raw until asked for
             if self.quad is not None:

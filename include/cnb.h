@@ -307,6 +307,16 @@ int cnb_upward_table_quad(const float *px, const float *py, const float *pz, con
                           float *node_table, float *sums, float *quad, int64_t n,
                           int32_t *status, void *stream);
 
+/* cnb_upward_table (quad NULL) or cnb_upward_table_quad, computed over the
+ * bucket table of cnb_make_buckets (buckets of at most 64 bodies; larger
+ * ones raise CNB_FLAG_LIST_OVERFLOW): one warp per bucket forms the nodes
+ * inside it with shared-memory counters, then one thread per bucket root
+ * climbs the levels above.  Same table, bit for bit. */
+int cnb_upward_table_buckets(const float *px, const float *py, const float *pz, const float *mass,
+                             const int32_t *children, const int32_t *parents,
+                             const int32_t *workspace, int32_t *counts, float *node_table,
+                             float *sums, float *quad, int64_t n, int32_t *status, void *stream);
+
 /* cnb_forces_grouped_boxes under the periodic law of cnb_forces_grouped_ewald:
  * every box is periodic on its own unit cube. */
 int cnb_forces_grouped_boxes_ewald(const float *px, const float *py, const float *pz,

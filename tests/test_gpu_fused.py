@@ -79,3 +79,51 @@ def test_octree_manager_grouped_buffers_are_reference_layout():
     np.testing.assert_array_equal(buf["com"].cpu().numpy(), wc)
     np.testing.assert_array_equal(buf["min"].cpu().numpy(), wlo)
     assert int(buf["root"].item()) == n
+
+
+@pytest.mark.parametrize("n_grid,bucket", [(2, 32), (16, 32), (32, 64), (24, 16)])
+def test_bucketed_upward_equals_one_pass(n_grid, bucket):
+    """cnb_upward_table_buckets (warp per bucket, shared-memory counters, then
+    the levels above) writes the same bits as the one-pass cnb_upward_table,
+    with and without second moments."""
+    from cnb import _lib
+    pos, codes = _tree(n_grid, 7)
+    n = codes.size
+    m = 2 * n - 1
+    st = int(torch.cuda.current_stream().cuda_stream)
+    K = torch.from_numpy(codes).cuda()
+    P = [torch.from_numpy(a).cuda() for a in pos]
+    M = torch.full((n,), 1.0 / n, device="cuda")
+    ch = torch.full((m, 2), -1, dtype=torch.int32, device="cuda")
+    par = torch.full((m,), -1, dtype=torch.int32, device="cuda")
+    rg = torch.zeros((max(n - 1, 1), 2), dtype=torch.int32, device="cuda")
+    _lib.call("cnb_build_tree_ranges", K.data_ptr(), ch.data_ptr(), par.data_ptr(), rg.data_ptr(), n, st)
+    ws = torch.zeros(4 + 4 * n, dtype=torch.int32, device="cuda")
+    _lib.call("cnb_make_buckets", rg.data_ptr(), par.data_ptr(), n, bucket, ws.data_ptr(), st)
+    for quad in (False, True):
+        out = []
+        for entry in ("one", "buckets"):
+            table = torch.zeros((4, m, 4), device="cuda")
+            sums = torch.zeros((m, 4), device="cuda")
+            q = torch.zeros((m, 8), device="cuda") if quad else None
+            counts = torch.zeros(m, dtype=torch.int32, device="cuda")
+            status = torch.zeros(1, dtype=torch.int32, device="cuda")
+            qp = q.data_ptr() if quad else None
+            if entry == "one" and quad:
+                _lib.call("cnb_upward_table_quad", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(),
+                          par.data_ptr(), counts.data_ptr(), table.data_ptr(), sums.data_ptr(), qp, n,
+                          status.data_ptr(), st)
+            elif entry == "one":
+                _lib.call("cnb_upward_table", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(),
+                          par.data_ptr(), counts.data_ptr(), table.data_ptr(), sums.data_ptr(), n,
+                          status.data_ptr(), st)
+            else:
+                _lib.call("cnb_upward_table_buckets", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(),
+                          par.data_ptr(), ws.data_ptr(), counts.data_ptr(), table.data_ptr(), sums.data_ptr(),
+                          qp, n, status.data_ptr(), st)
+            torch.cuda.synchronize()
+            assert int(status.item()) == 0
+            out.append((table.cpu().numpy(), q.cpu().numpy()[n:] if quad else None))
+        np.testing.assert_array_equal(out[0][0].view(np.uint32), out[1][0].view(np.uint32))
+        if quad:
+            np.testing.assert_array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))
