@@ -68,7 +68,7 @@ __device__ __forceinline__ void form_node(int64_t p, int2 ch, bool mine_left, fl
                                           float4 &lo, float4 &hi, float4 &qa, float4 &qb,
                                           float4 bs, float4 blo, float4 bhi, float4 ba,
                                           float4 bb, float4 *sums, float4 *rec, float4 *aabb,
-                                          float4 *quad) {
+                                          float4 *quad, bool keep_sums = true) {
     const float4 &Ls = mine_left ? s : bs, &Rs = mine_left ? bs : s;
     const float4 &Llo = mine_left ? lo : blo, &Rlo = mine_left ? blo : lo;
     const float4 &Lhi = mine_left ? hi : bhi, &Rhi = mine_left ? bhi : hi;
@@ -76,7 +76,7 @@ __device__ __forceinline__ void form_node(int64_t p, int2 ch, bool mine_left, fl
                                   __fadd_rn(Ls.z, Rs.z), __fadd_rn(Ls.w, Rs.w));
     const float4 qlo = make_float4(umin(Llo.x, Rlo.x), umin(Llo.y, Rlo.y), umin(Llo.z, Rlo.z), 0.f);
     const float4 qhi = make_float4(umax(Lhi.x, Rhi.x), umax(Lhi.y, Rhi.y), umax(Lhi.z, Rhi.z), 0.f);
-    sums[p] = qs;
+    if (keep_sums) sums[p] = qs;  // the raw sums are read again only by climbs
     store_record(rec, aabb, p, qs, qlo, qhi, ch.x, ch.y);
     if (QUAD) {
         // left child first, then right: the same bits whichever child arrives second
@@ -215,7 +215,8 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_buckets(
             float4 s = make_float4(__fmul_rn(x, m), __fmul_rn(y, m), __fmul_rn(z, m), m);
             float4 lo = make_float4(x, y, z, 0.f), hi = lo;
             float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;
-            sums[i] = s;
+            // raw sums go to global memory only for the bucket root (phase two reads them)
+            if (i == root) sums[i] = s;
             store_record(rec, aabb, i, s, lo, hi, -1, -1);
             s_sum[w][k] = s;
             s_lo[w][k] = lo;
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_buckets(
                     bb = s_qb[w][so];
                 }
                 form_node<QUAD>(p, ch, mine_left, s, lo, hi, qa, qb, bs, blo, bhi, ba, bb, sums, rec,
-                                aabb, quad);
+                                aabb, quad, p == root);
                 const int ns = kUpSlots + (int)ps;
                 s_sum[w][ns] = s;
                 s_lo[w][ns] = lo;

@@ -311,7 +311,8 @@ int cnb_upward_table_quad(const float *px, const float *py, const float *pz, con
  * bucket table of cnb_make_buckets (buckets of at most 64 bodies; larger
  * ones raise CNB_FLAG_LIST_OVERFLOW): one warp per bucket forms the nodes
  * inside it with shared-memory counters, then one thread per bucket root
- * climbs the levels above.  Same table, bit for bit. */
+ * climbs the levels above.  Same table, bit for bit; sums (climb scratch)
+ * then holds raw sums only for bucket roots and the nodes above them. */
 int cnb_upward_table_buckets(const float *px, const float *py, const float *pz, const float *mass,
                              const int32_t *children, const int32_t *parents,
                              const int32_t *workspace, int32_t *counts, float *node_table,
