@@ -254,9 +254,10 @@ __global__ void __launch_bounds__(kSortThreads) k_digit_hist_all(const uint64_t 
 // count of this and every earlier tile).
 constexpr uint64_t kLbCount = 1ull << 32, kLbPrefix = 2ull << 32;
 // the one-sweep tile and how many earlier tiles one look-back step reads
-constexpr int kSweepItems = 16;
+constexpr int kSweepThreads = 512;  // 16 warps: a short ranking chain, 32 warps per SM
+constexpr int kSweepItems = 8;
 constexpr int kLookbackWindow = 4;
-constexpr int kSweepTile = kSortThreads * kSweepItems;
+constexpr int kSweepTile = kSweepThreads * kSweepItems;
 constexpr int kSweepSmem = kSweepTile * (sizeof(uint64_t) + sizeof(uint32_t));
 static_assert(kSweepTile >= 2048, "sweep_bytes() sizes the look-back words for 2048-key tiles");
 constexpr int kLookbackSpinLimit = 1 << 22;
@@ -270,8 +271,27 @@ __device__ __forceinline__ uint64_t lb_load(const uint64_t *p) {
     return v;
 }
 
+// Exclusive scan over the NT threads of a block (one value each).
+template <int NT>
+__device__ __forceinline__ uint32_t block_exscan(uint32_t v, uint32_t *warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_sums[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+#pragma unroll
+    for (int w = 0; w < NT / 32; ++w) wbase += (w < warp) ? warp_sums[w] : 0u;
+    __syncthreads();
+    return wbase + incl - v;
+}
+
 template <bool IDENTITY_IN>
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t *__restrict__ kin,
+__global__ void __launch_bounds__(kSweepThreads) k_onesweep(const uint64_t *__restrict__ kin,
                                                            const uint32_t *__restrict__ vin,
                                                            uint64_t *__restrict__ kout,
                                                            uint32_t *__restrict__ vout,
@@ -280,22 +300,23 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t *__res
                                                            uint64_t *lookback,
                                                            int32_t *tile_counter,
                                                            int32_t *flags) {
-    static_assert(kSortThreads == 256, "block scans assume 256 threads");
-    constexpr int W = kSortThreads / 32;
+    static_assert(kSweepThreads >= 256, "one thread per digit");
+    constexpr int W = kSweepThreads / 32;
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *skey = reinterpret_cast<uint64_t *>(smem);
     uint32_t *sval = reinterpret_cast<uint32_t *>(smem + kSweepTile * sizeof(uint64_t));
     __shared__ uint32_t wcnt[W][257];
     __shared__ uint32_t gbase[256];
     __shared__ uint32_t tstart[256];
-    __shared__ uint32_t wsum[8];
+    __shared__ uint32_t wsum[W];
     __shared__ int s_tile;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool digit_thread = threadIdx.x < 256;
     // tiles in the order blocks start: every tile this one waits for has started
     if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1);
-    for (int i = threadIdx.x; i < W * 257; i += kSortThreads) (&wcnt[0][0])[i] = 0;
-    // start of each digit among all keys
-    const uint32_t digit_start = block_exscan256(hist[threadIdx.x], wsum);
+    for (int i = threadIdx.x; i < W * 257; i += kSweepThreads) (&wcnt[0][0])[i] = 0;
+    // start of each digit among all keys (threads 0..255, one digit each)
+    const uint32_t digit_start = block_exscan<kSweepThreads>(digit_thread ? hist[threadIdx.x] : 0u, wsum);
     __syncthreads();
     const int64_t tile = s_tile;
 
@@ -328,53 +349,56 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t *__res
     {
         const int d = threadIdx.x;
         uint32_t run = 0;
-#pragma unroll
-        for (int w = 0; w < W; ++w) {
-            const uint32_t c = wcnt[w][d];
-            wcnt[w][d] = run;
-            run += c;
-        }
-        // publish this tile's count, then add up the earlier tiles' counts
-        uint64_t *mine = lookback + tile * 256 + d;
         uint32_t before = 0;
-        if (tile == 0) {
-            lb_store(mine, kLbPrefix | run);
-        } else {
-            lb_store(mine, kLbCount | run);
-            // kLookbackWindow earlier tiles per round trip, used in order up
-            // to the first one not yet published (tile 0 always ends the walk)
-            int64_t j = tile - 1;
-            int spins = 0;
-            for (;;) {
-                uint64_t v[kLookbackWindow];
+        if (digit_thread) {
 #pragma unroll
-                for (int w = 0; w < kLookbackWindow; ++w)
-                    v[w] = (j - w >= 0) ? lb_load(lookback + (j - w) * 256 + d) : kLbPrefix;
-                int used = 0;
-                bool done = false;
-#pragma unroll
-                for (int w = 0; w < kLookbackWindow; ++w) {
-                    const uint32_t state = (uint32_t)(v[w] >> 32);
-                    if (!done && used == w && state != 0) {
-                        before += (uint32_t)v[w];
-                        used = w + 1;
-                        done = (state == 2);
-                    }
-                }
-                if (done) break;
-                j -= used;
-                if (used == 0) {
-                    if (++spins > kLookbackSpinLimit) {
-                        set_flag(flags, CNB_FLAG_WAIT_LIMIT);
-                        break;
-                    }
-                    if (spins > 16) __nanosleep(64);
-                }
+            for (int w = 0; w < W; ++w) {
+                const uint32_t c = wcnt[w][d];
+                wcnt[w][d] = run;
+                run += c;
             }
-            lb_store(mine, kLbPrefix | (before + run));
+            // publish this tile's count, then add up the earlier tiles' counts
+            uint64_t *mine = lookback + tile * 256 + d;
+            if (tile == 0) {
+                lb_store(mine, kLbPrefix | run);
+            } else {
+                lb_store(mine, kLbCount | run);
+                // kLookbackWindow earlier tiles per round trip, used in order up
+                // to the first one not yet published (tile 0 always ends the walk)
+                int64_t j = tile - 1;
+                int spins = 0;
+                for (;;) {
+                    uint64_t v[kLookbackWindow];
+#pragma unroll
+                    for (int w = 0; w < kLookbackWindow; ++w)
+                        v[w] = (j - w >= 0) ? lb_load(lookback + (j - w) * 256 + d) : kLbPrefix;
+                    int used = 0;
+                    bool done = false;
+#pragma unroll
+                    for (int w = 0; w < kLookbackWindow; ++w) {
+                        const uint32_t state = (uint32_t)(v[w] >> 32);
+                        if (!done && used == w && state != 0) {
+                            before += (uint32_t)v[w];
+                            used = w + 1;
+                            done = (state == 2);
+                        }
+                    }
+                    if (done) break;
+                    j -= used;
+                    if (used == 0) {
+                        if (++spins > kLookbackSpinLimit) {
+                            set_flag(flags, CNB_FLAG_WAIT_LIMIT);
+                            break;
+                        }
+                        if (spins > 16) __nanosleep(64);
+                    }
+                }
+                lb_store(mine, kLbPrefix | (before + run));
+            }
+            gbase[d] = digit_start + before;
         }
-        gbase[d] = digit_start + before;
-        tstart[d] = block_exscan256(run, wsum);
+        const uint32_t ts = block_exscan<kSweepThreads>(run, wsum);
+        if (digit_thread) tstart[d] = ts;
     }
     __syncthreads();
 #pragma unroll
@@ -389,7 +413,7 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t *__res
     }
     __syncthreads();
     const int tile_n = (int)min((int64_t)kSweepTile, n - tbase);
-    for (int j = threadIdx.x; j < tile_n; j += kSortThreads) {
+    for (int j = threadIdx.x; j < tile_n; j += kSweepThreads) {
         const uint64_t k = skey[j];
         const uint32_t d = (uint32_t)(k >> shift) & 255u;
         const int64_t pos = (int64_t)gbase[d] + (j - tstart[d]);
@@ -434,10 +458,10 @@ int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_ou
         uint32_t *vd = last ? perm_out : ctx->vals_tmp[p & 1];
         uint64_t *lb = lookback + (int64_t)p * tiles * 256;
         if (vs == nullptr)
-            k_onesweep<true><<<(unsigned)tiles, kSortThreads, kSweepSmem, st>>>(
+            k_onesweep<true><<<(unsigned)tiles, kSweepThreads, kSweepSmem, st>>>(
                 ks, nullptr, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags);
         else
-            k_onesweep<false><<<(unsigned)tiles, kSortThreads, kSweepSmem, st>>>(
+            k_onesweep<false><<<(unsigned)tiles, kSweepThreads, kSweepSmem, st>>>(
                 ks, vs, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags);
         CNB_TRY(launch_status());
         ks = kd;

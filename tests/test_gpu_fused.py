@@ -127,3 +127,54 @@ def test_bucketed_upward_equals_one_pass(n_grid, bucket):
         np.testing.assert_array_equal(out[0][0].view(np.uint32), out[1][0].view(np.uint32))
         if quad:
             np.testing.assert_array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))
+
+
+def test_bucketed_upward_flags_corrupted_topology():
+    """Faults made on the host in a valid tree: a node that is its own parent,
+    a leaf whose parent lies outside its bucket, and a bucket above the 64
+    bodies the shared-memory pass handles.  Every climb is bounded, so each
+    ends with a flag instead of a hang."""
+    from cnb import _lib
+    pos, codes = _tree(16, 8)
+    n = codes.size
+    m = 2 * n - 1
+    st = int(torch.cuda.current_stream().cuda_stream)
+    K = torch.from_numpy(codes).cuda()
+    P = [torch.from_numpy(a).cuda() for a in pos]
+    M = torch.full((n,), 1.0 / n, device="cuda")
+    ch = torch.full((m, 2), -1, dtype=torch.int32, device="cuda")
+    par0 = torch.full((m,), -1, dtype=torch.int32, device="cuda")
+    rg = torch.zeros((n - 1, 2), dtype=torch.int32, device="cuda")
+    _lib.call("cnb_build_tree_ranges", K.data_ptr(), ch.data_ptr(), par0.data_ptr(), rg.data_ptr(), n, st)
+    ws = torch.zeros(4 + 4 * n, dtype=torch.int32, device="cuda")
+    _lib.call("cnb_make_buckets", rg.data_ptr(), par0.data_ptr(), n, 64, ws.data_ptr(), st)
+    torch.cuda.synchronize()
+    bk = ws[4:4 + 4 * int(ws[0].item())].view(-1, 4).cpu().numpy()
+    big = bk[np.argmax(bk[:, 1])]
+    assert big[1] >= 2
+
+    def run(par, work):
+        status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        _lib.call("cnb_upward_table_buckets", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(),
+                  par.data_ptr(), work.data_ptr(), torch.zeros(m, dtype=torch.int32, device="cuda").data_ptr(),
+                  torch.zeros((4, m, 4), device="cuda").data_ptr(), torch.zeros((m, 4), device="cuda").data_ptr(),
+                  None, n, status.data_ptr(), st)
+        torch.cuda.synchronize()
+        return int(status.item())
+
+    assert run(par0, ws) == 0
+    # an internal node of a bucket that is its own parent
+    par = par0.clone()
+    inner = int(par0[int(big[0])].item())
+    par[inner] = inner
+    assert run(par, ws) & _lib.FLAG_BAD_TOPOLOGY
+    # a leaf whose parent lies outside its bucket
+    par = par0.clone()
+    par[int(big[0])] = n  # the tree's root: not in any bucket of several bodies
+    assert run(par, ws) & _lib.FLAG_BAD_TOPOLOGY
+    # a bucket table with buckets of up to 128 bodies
+    ws128 = torch.zeros_like(ws)
+    _lib.call("cnb_make_buckets", rg.data_ptr(), par0.data_ptr(), n, 128, ws128.data_ptr(), st)
+    torch.cuda.synchronize()
+    if int(ws128[4:4 + 4 * int(ws128[0].item())].view(-1, 4)[:, 1].max().item()) > 64:
+        assert run(par0, ws128) & _lib.FLAG_LIST_OVERFLOW
