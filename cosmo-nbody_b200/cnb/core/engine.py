@@ -80,6 +80,8 @@ class SimulationEngine:
             self.set_super_bodies(int(getattr(config, "SUPER_BODIES", 0)))
         self.precision = _lib.PREC_F64 if getattr(config, "PRECISION", "f32") == "f64" else _lib.PREC_F32
         self.stage_events = None
+        self.nvtx = False          # NVTX ranges around the step's stages (for nsys / ncu timelines)
+        self._nvtx_open = False
 
     def set_super_bodies(self, super_bodies):
         """Two-level walk with super-buckets of at most `super_bodies` bodies
@@ -143,11 +145,22 @@ class SimulationEngine:
                       float(cfg.THETA), float(cfg.G), float(cfg.SOFTENING), float(cfg.BOX_SIZE),
                       tm.root_idx.data_ptr(), 0, s.n, s.n, self.precision, status, st)
 
+    _NEXT_STAGE = {"start": "sort", "sort": "tree", "tree": "forces"}
+
     def _mark(self, name):
         if self.stage_events is not None:
             ev = torch.cuda.Event(enable_timing=True)
             ev.record()
             self.stage_events.append((name, ev))
+        if self.nvtx:
+            # a mark ends the stage named after it and opens the next one
+            if self._nvtx_open:
+                torch.cuda.nvtx.range_pop()
+                self._nvtx_open = False
+            nxt = self._NEXT_STAGE.get(name)
+            if nxt is not None:
+                torch.cuda.nvtx.range_push(nxt)
+                self._nvtx_open = True
 
     def forces_only(self):
         """Sort, tree and forces for the current state (no integration)."""
@@ -164,6 +177,9 @@ class SimulationEngine:
         H = get_hubble_param(self.a, self.config)
         dt_physics = self.da / (self.a * H) * 0.8
         self.forces_only()
+        if self.nvtx:
+            torch.cuda.nvtx.range_push("integrate")
+            self._nvtx_open = True
         s = self.state
         _lib.call("cnb_integrate", *(t.data_ptr() for t in s.pos + s.vel), s.force.data_ptr(), s.n,
                   float(self.a), float(H), float(dt_physics), self._stream())
@@ -234,6 +250,27 @@ class SimulationEngine:
         self._graph.replay()
         self._graph_step += 2
         self.a += 2 * self.da
+
+    def save_state(self, path):
+        """Checkpoint: positions, velocities, masses, the scale factor and
+        the camera step, as one torch file (resume with load_state)."""
+        s = self.state
+        torch.save({"n": s.n, "pos": [p.cpu() for p in s.pos], "vel": [v.cpu() for v in s.vel],
+                    "mass": s.mass.cpu(), "a": float(self.a),
+                    "graph_step": int(getattr(self, "_graph_step", 0))}, path)
+
+    def load_state(self, path):
+        """Resume from save_state: the arrays are copied into this engine's
+        buffers (the body count must match)."""
+        d = torch.load(path)
+        s = self.state
+        if int(d["n"]) != s.n:
+            raise ValueError(f"checkpoint has {d['n']} bodies, the engine {s.n}")
+        for dst, src in zip(s.pos + s.vel, d["pos"] + d["vel"]):
+            dst.copy_(src)
+        s.mass.copy_(d["mass"])
+        self.a = float(d["a"])
+        self._graph = None    # a captured graph holds the old scalars
 
     def enable_stage_timing(self, on=True):
         """Record CUDA events between the stages of every step (stage_times() reads them)."""

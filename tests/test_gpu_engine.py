@@ -330,3 +330,69 @@ def test_device_initial_conditions_match_host_generator():
             ulp = np.spacing(np.abs(h)).astype(np.float64)
             assert np.all(np.abs(d.astype(np.float64) - h) <= ulp)
             assert np.mean(d == h) > 0.99
+
+
+def test_checkpoint_resume_and_nvtx_ranges(tmp_path):
+    """save_state / load_state: a run resumed from a checkpoint continues
+    exactly like the uninterrupted run; NVTX ranges do not change results."""
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = config(16, KEY_MODE="morton63", FORCE_MODE="grouped")
+    pos, vel = zeldovich_arrays(16, 3)
+    a_eng = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel), camera=False)
+    a_eng.nvtx = True
+    for _ in range(2):
+        a_eng.step()
+    path = str(tmp_path / "state.pt")
+    a_eng.save_state(path)
+    a_saved = a_eng.a
+    for _ in range(2):
+        a_eng.step()
+    b_eng = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel), camera=False)
+    b_eng.load_state(path)
+    assert b_eng.a == a_saved
+    for _ in range(2):
+        b_eng.step()
+    a_eng.check()
+    b_eng.check()
+    for x, y in zip(a_eng.state.pos + a_eng.state.vel, b_eng.state.pos + b_eng.state.vel):
+        np.testing.assert_array_equal(host(x), host(y))
+    c_eng = SimulationEngine(config(8, KEY_MODE="morton63", FORCE_MODE="grouped"),
+                             SimulationState(8 ** 3, *zeldovich_arrays(8, 3)), camera=False)
+    with pytest.raises(ValueError):
+        c_eng.load_state(path)
+
+
+def test_reference_traversal_flags_stack_overflow():
+    """A chain-shaped tree deeper than the reference's 64-entry DFS stack
+    (made on the host): the reference drops children silently; this
+    traversal drops them too, flags CNB_FLAG_STACK_OVERFLOW and ends."""
+    from cnb import _lib
+    n = 200
+    m = 2 * n - 1
+    # internal node n + k has children (internal n + k + 1, leaf k): the walk
+    # pops the internal child first and leaves one leaf per level on the
+    # stack; the last internal node has two leaves (depth n - 1)
+    children = np.full((m, 2), -1, np.int32)
+    for k in range(n - 1):
+        children[n + k] = (n + k + 1, k) if k < n - 2 else (k, k + 1)
+    rng = np.random.default_rng(0)
+    pos = rng.random((n, 3)).astype(np.float32)
+    n_mass = np.full(m, 1.0 / n, np.float32)
+    n_com = np.concatenate([pos, np.full((n - 1, 3), 0.5, np.float32)])
+    n_min = np.concatenate([pos, np.zeros((n - 1, 3), np.float32)])
+    n_max = np.concatenate([pos, np.ones((n - 1, 3), np.float32)])
+    d = lambda a: torch.from_numpy(np.ascontiguousarray(a)).cuda()
+    P = [d(pos[:, i]) for i in range(3)]
+    # the device copies stay referenced until the kernels have run
+    tree = [d(children), d(n_mass), d(n_com), d(n_min), d(n_max)]
+    root = torch.tensor([n], dtype=torch.int32, device="cuda")
+    f = torch.zeros((n, 3), device="cuda")
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    for prec in (_lib.PREC_F32, _lib.PREC_F64):
+        status.zero_()
+        _lib.call("cnb_compute_forces", *(p.data_ptr() for p in P), *(t.data_ptr() for t in tree),
+                  f.data_ptr(), 0.0, 1.0, 0.01, 1.0, root.data_ptr(), 0, n, n, prec, status.data_ptr(),
+                  int(torch.cuda.current_stream().cuda_stream))
+        assert int(host(status)[0]) & _lib.FLAG_STACK_OVERFLOW

@@ -154,10 +154,13 @@ def test_bucketed_upward_flags_corrupted_topology():
     assert big[1] >= 2
 
     def run(par, work):
+        # every buffer stays referenced until the kernels have run
         status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        counts = torch.zeros(m, dtype=torch.int32, device="cuda")
+        table = torch.zeros((4, m, 4), device="cuda")
+        sums = torch.zeros((m, 4), device="cuda")
         _lib.call("cnb_upward_table_buckets", *(p.data_ptr() for p in P), M.data_ptr(), ch.data_ptr(),
-                  par.data_ptr(), work.data_ptr(), torch.zeros(m, dtype=torch.int32, device="cuda").data_ptr(),
-                  torch.zeros((4, m, 4), device="cuda").data_ptr(), torch.zeros((m, 4), device="cuda").data_ptr(),
+                  par.data_ptr(), work.data_ptr(), counts.data_ptr(), table.data_ptr(), sums.data_ptr(),
                   None, n, status.data_ptr(), st)
         torch.cuda.synchronize()
         return int(status.item())
