@@ -28,7 +28,19 @@
 //                     the per-pair minimum image of its CoM.  slab_mass = 0 is
 //                     exact; a small positive value bounds the cost of the
 //                     sources near the plane antipodal to the bucket.
+//   CNB_MAC_EWALD:    the periodic (Ewald) force law (the EWALD variant of the
+//                     kernel): 3-D extent, or b_max with quadrupoles; every
+//                     accepted node at the image nearest the bucket centre for
+//                     the whole bucket, plus the periodic correction of every
+//                     accepted node, accumulated per lane while walking and
+//                     applied per body once per bucket (ewald.cu has the law).
+//                     With quadrupole moments the second list carries the
+//                     internal nodes with their second central moments.
 // theta is one value or one per bucket (learned controller).
+//
+// Two bodies per lane run the force loop on packed float2 (FADD2 / FMUL2 /
+// FFMA2); the two-level walk (k_super_lists, cnb_forces_two_level) lets a
+// super-bucket walk the top of the tree once for all its buckets.
 #include "common.cuh"
 
 namespace cnb {
