@@ -10,7 +10,7 @@ import numpy as np
 import torch
 
 from ._lib import CnbError, FLAG_BAD_TOPOLOGY, FLAG_LIST_OVERFLOW, FLAG_NONFINITE, \
-    FLAG_STACK_OVERFLOW, FLAG_WAIT_LIMIT
+    FLAG_SORT_CHECK, FLAG_STACK_OVERFLOW, FLAG_WAIT_LIMIT
 
 _TYPESTR = {
     np.dtype(np.float32): "<f4",
@@ -93,6 +93,7 @@ FLAG_NAMES = {
     FLAG_NONFINITE: "non-finite acceleration",
     FLAG_LIST_OVERFLOW: "grouped traversal work queue exhausted",
     FLAG_WAIT_LIMIT: "a bounded wait between blocks gave up (sort result invalid)",
+    FLAG_SORT_CHECK: "a destination check of the near-sorted sort failed (sort result invalid)",
 }
 
 
@@ -110,7 +111,8 @@ def read_status(device=None, clear=True):
 
 
 def check_status(device=None,
-                 fatal=FLAG_BAD_TOPOLOGY | FLAG_NONFINITE | FLAG_LIST_OVERFLOW | FLAG_WAIT_LIMIT):
+                 fatal=FLAG_BAD_TOPOLOGY | FLAG_NONFINITE | FLAG_LIST_OVERFLOW | FLAG_WAIT_LIMIT |
+                       FLAG_SORT_CHECK):
     """Raise CnbError if a fatal flag was raised since the last check."""
     val = read_status(device)
     if val & fatal:

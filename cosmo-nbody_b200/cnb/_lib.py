@@ -24,12 +24,16 @@ FLAG_BAD_TOPOLOGY = 2
 FLAG_NONFINITE = 4
 FLAG_LIST_OVERFLOW = 8
 FLAG_WAIT_LIMIT = 16
+FLAG_SORT_CHECK = 32
 
 KEY_COMPAT30 = 0
 KEY_MORTON63 = 1
 MAC_REF_X = 0
 MAC_PERIODIC = 1
 MAC_EWALD = 2
+SORT_FULL = 0
+SORT_ADAPTIVE = 1
+SORT_NEAR_CAP = 2048
 PREC_F32 = 0
 PREC_F64 = 1
 UPWARD_PLAIN = 0
@@ -54,6 +58,8 @@ SIGNATURES = {
     "cnb_ctx_destroy": (_int, [_p]),
     "cnb_sort_pairs": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
     "cnb_sort_pairs_noalloc": (_int, [_p, _p, _p, _p, _i64, _int, _p]),
+    "cnb_ctx_set_sort_mode": (_int, [_p, _int]),
+    "cnb_ctx_sort_stats": (_int, [_p, _p]),
     "cnb_ctx_take_flags": (_int, [_p, _p, _p]),
     "cnb_gather_f32": (_int, [_p, _int, _p, _p, _i64, _p]),
     "cnb_reset_tree_buffers": (_int, [_p, _p, _p, _p, _i64, _p]),

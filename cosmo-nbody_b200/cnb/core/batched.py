@@ -115,6 +115,8 @@ class BatchedBoxes:
             self.ewald_table = z((EWALD_NT + 1) ** 3, 24)
             _lib.call("cnb_ewald_table", self.ewald_table.data_ptr(), EWALD_NT, self._st())
         self._ctx = SortContext(n)
+        # full Morton keys below the box bits: the previous step's order mostly holds
+        self._ctx.set_mode("adaptive")
         self._graph = None
 
     # ------------------------------------------------------------ step parts

@@ -10,6 +10,11 @@ once, here.
 `sort_buffer_by_morton(config)` computes the keys (config.KEY_MODE,
 "compat30" by default = the reference's keys), sorts (key, index) pairs with
 libcnb's stable radix sort and gathers positions, velocities and masses.
+config.SORT_MODE picks the sort: "full" (the radix sort every step),
+"adaptive" (the near-sorted path first: keys that were sorted one step
+earlier mostly keep their order; the result is the same argsort) or "auto"
+(adaptive for "morton63" keys, full for "compat30" keys, whose low 10 bits
+per axis reorder at every step).
 Like the reference it rebinds `pos`, `vel`, `mass` and `codes` to the sorted
 arrays; the arrays alternate between two preallocated sets, so no memory is
 allocated per step.
@@ -24,6 +29,19 @@ import torch
 from .. import _lib
 from .._arrays import status_buffer
 from ..kernels.morton import KEY_BITS, KEY_MODES
+
+
+SORT_MODES = {"full": _lib.SORT_FULL, "adaptive": _lib.SORT_ADAPTIVE}
+
+
+def sort_mode_for(config, key_mode):
+    """The SORT_MODES name config.SORT_MODE selects for keys of key_mode."""
+    mode = getattr(config, "SORT_MODE", "auto")
+    if mode == "auto":
+        return "adaptive" if key_mode == "morton63" else "full"
+    if mode not in SORT_MODES:
+        raise ValueError(f"SORT_MODE must be 'auto', 'full' or 'adaptive', got {mode!r}")
+    return mode
 
 
 def _to_device_f32(a, device):
@@ -50,6 +68,18 @@ class SortContext:
         if status is None:
             status = status_buffer().data_ptr()
         _lib.call("cnb_ctx_take_flags", self.ptr, status, stream)
+
+    def set_mode(self, mode):
+        """SORT_MODES name: "full" radix sort every call, or "adaptive"
+        (near-sorted path first, full sort only when it does not apply)."""
+        _lib.call("cnb_ctx_set_sort_mode", self.ptr, SORT_MODES[mode])
+
+    def stats(self):
+        """(sorts that took the near-sorted path, full radix sorts run);
+        synchronises the device."""
+        out = (C.c_int64 * 2)()
+        _lib.call("cnb_ctx_sort_stats", self.ptr, out)
+        return int(out[0]), int(out[1])
 
     def close(self):
         if self.ptr:
@@ -103,6 +133,7 @@ class SimulationState:
             return
         if self._ctx is None:
             self._ctx = SortContext(self.n)
+        self._ctx.set_mode(sort_mode_for(config, key_mode))
         st = self._stream()
         p = self.pos
         _lib.call("cnb_compute_codes", p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(),

@@ -37,6 +37,8 @@ STACK_SIZE_CHILD = 128
 
 # --- B200 step options (no reference counterpart) ---
 KEY_MODE = "compat30"      # "compat30": reference keys, bit-exact; "morton63": full 21-bit interleave
+SORT_MODE = "auto"         # "full": radix sort every step; "adaptive": near-sorted path first (same
+                           # argsort); "auto": adaptive for morton63 keys, full for compat30 keys
 FORCE_MODE = "reference"   # "reference": per-particle stack traversal; "grouped": warp-per-bucket traversal
 MAC = "ref_x"              # "ref_x": reference opening test; "periodic": 3-D extent + image-safe opening;
                            # "ewald": periodic (Ewald) force law instead of the minimum image, 3-D extent

@@ -15,12 +15,28 @@ struct cnb_ctx {
     // then the look-back words of every pass, [8 x tiles x 256] (2048-key tiles)
     uint32_t *sweep = nullptr;
     int32_t *flags = nullptr;       // CNB_FLAG_* raised by the sort, taken by cnb_ctx_take_flags
+    // near-sorted path of the adaptive sort (sort_near.cu): one allocation
+    int sort_mode = CNB_SORT_FULL;
+    void *near = nullptr;
+    unsigned long long *sort_stats = nullptr;  // [near-sorted path taken, full radix sorts run]
     // grouped traversal scratch (grown on demand by cnb_forces_grouped)
     void *group_scratch = nullptr;
     size_t group_scratch_bytes = 0;
 };
 
 namespace cnb {
+// tiles and the bound on out-of-place keys of the near-sorted path
+constexpr int kNearThreads = 512;
+constexpr int kNearItems = 8;
+constexpr int kNearTile = kNearThreads * kNearItems;  // 4096 keys
+constexpr int kNearCap = 2048;                        // at most this many keys leave their run
+int64_t near_bytes(int64_t n_max);
+int sort_pairs_near(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
+                    uint32_t *perm_out, int64_t n, cudaStream_t st, const int32_t **skip_full);
+int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
+                        const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
+                        cudaStream_t st, const int32_t *skip = nullptr);
+
 constexpr int kSortThreads = 256;
 constexpr int kSortItems = 16;
 constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile

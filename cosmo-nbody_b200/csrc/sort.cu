@@ -211,10 +211,17 @@ __global__ void __launch_bounds__(kSortThreads) k_scatter(const uint64_t *__rest
 // Counts of every digit of the first `passes` passes.  Each thread sums
 // runs of equal digits over kSortItems consecutive keys before touching the
 // shared histograms (sorted or nearly sorted input repeats its high digits).
+// skip: a device flag set when the near-sorted path already produced the
+// result (every kernel of the full sort then returns at once); runs: counts
+// the full sorts that ran.
 __global__ void __launch_bounds__(kSortThreads) k_digit_hist_all(const uint64_t *__restrict__ keys,
                                                                  int64_t n, int passes,
-                                                                 uint32_t *__restrict__ hist) {
+                                                                 uint32_t *__restrict__ hist,
+                                                                 const int32_t *skip,
+                                                                 unsigned long long *runs) {
     __shared__ uint32_t sh[kSweepPasses][256];
+    if (skip && *(volatile const int32_t *)skip) return;
+    if (runs && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(runs, 1ull);
     for (int i = threadIdx.x; i < kSweepPasses * 256; i += kSortThreads) (&sh[0][0])[i] = 0;
     __syncthreads();
     for (int64_t base = ((int64_t)blockIdx.x * kSortThreads + threadIdx.x) * kSortItems; base < n;
@@ -299,8 +306,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_onesweep(const uint64_t *__re
                                                            const uint32_t *__restrict__ hist,
                                                            uint64_t *lookback,
                                                            int32_t *tile_counter,
-                                                           int32_t *flags) {
+                                                           int32_t *flags, const int32_t *skip) {
     static_assert(kSweepThreads >= 256, "one thread per digit");
+    if (skip && *(volatile const int32_t *)skip) return;
     constexpr int W = kSweepThreads / 32;
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *skey = reinterpret_cast<uint64_t *>(smem);
@@ -422,6 +430,14 @@ __global__ void __launch_bounds__(kSweepThreads) k_onesweep(const uint64_t *__re
     }
 }
 
+__global__ void __launch_bounds__(256) k_zero_words(uint64_t *p, int64_t words,
+                                                    const int32_t *skip) {
+    if (*(volatile const int32_t *)skip) return;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < words;
+         i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = 0ull;
+}
+
 __global__ void k_take_flags(int32_t *ctx_flags, int32_t *status) {
     const int32_t f = *ctx_flags;
     if (f) {
@@ -432,7 +448,7 @@ __global__ void k_take_flags(int32_t *ctx_flags, int32_t *status) {
 
 int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                         const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
-                        cudaStream_t st) {
+                        cudaStream_t st, const int32_t *skip) {
     if (n == 0) return CNB_OK;
     int passes = (key_bits + 7) / 8;
     if (passes < 1) passes = 1;
@@ -441,14 +457,23 @@ int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_ou
     uint32_t *hist = ctx->sweep;
     int32_t *counters = reinterpret_cast<int32_t *>(ctx->sweep + kSweepPasses * 256);
     uint64_t *lookback = reinterpret_cast<uint64_t *>(ctx->sweep + kSweepMetaWords);
-    CNB_CUDA(cudaMemsetAsync(ctx->sweep, 0,
-                             kSweepMetaWords * 4 + (size_t)passes * tiles * 256 * 8, st));
+    const size_t zero_bytes = kSweepMetaWords * 4 + (size_t)passes * tiles * 256 * 8;
+    if (skip) {
+        // zeroed on the device only when this sort runs
+        static_assert((kSweepMetaWords * 4) % 8 == 0, "whole 64-bit words");
+        const int64_t words = (int64_t)(zero_bytes / 8);
+        k_zero_words<<<grid_for(words, 256, 148 * 8), 256, 0, st>>>(
+            reinterpret_cast<uint64_t *>(ctx->sweep), words, skip);
+        CNB_TRY(launch_status());
+    } else {
+        CNB_CUDA(cudaMemsetAsync(ctx->sweep, 0, zero_bytes, st));
+    }
     CNB_CUDA(cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kSweepSmem));
     CNB_CUDA(cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   kSweepSmem));
-    k_digit_hist_all<<<grid_for(n, kSortTile, 148 * 8), kSortThreads, 0, st>>>(keys_in, n, passes,
-                                                                              hist);
+    k_digit_hist_all<<<grid_for(n, kSortTile, 148 * 8), kSortThreads, 0, st>>>(
+        keys_in, n, passes, hist, skip, ctx->sort_stats ? ctx->sort_stats + 1 : nullptr);
     CNB_TRY(launch_status());
     const uint64_t *ks = keys_in;
     const uint32_t *vs = idx_in;
@@ -459,10 +484,10 @@ int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_ou
         uint64_t *lb = lookback + (int64_t)p * tiles * 256;
         if (vs == nullptr)
             k_onesweep<true><<<(unsigned)tiles, kSweepThreads, kSweepSmem, st>>>(
-                ks, nullptr, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags);
+                ks, nullptr, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags, skip);
         else
             k_onesweep<false><<<(unsigned)tiles, kSweepThreads, kSweepSmem, st>>>(
-                ks, vs, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags);
+                ks, vs, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags, skip);
         CNB_TRY(launch_status());
         ks = kd;
         vs = vd;
@@ -563,6 +588,9 @@ extern "C" int cnb_ctx_create(int64_t n_max, cnb_ctx **out) {
     if (e == cudaSuccess) e = cudaMalloc(&c->sweep, cnb::sweep_bytes(nn));
     if (e == cudaSuccess) e = cudaMalloc(&c->flags, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(c->flags, 0, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&c->near, cnb::near_bytes(nn));
+    if (e == cudaSuccess) e = cudaMalloc(&c->sort_stats, 2 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(c->sort_stats, 0, 2 * sizeof(unsigned long long));
     if (e != cudaSuccess) {
         cnb_ctx_destroy(c);
         cnb::record_cuda_error(e);
@@ -581,6 +609,8 @@ extern "C" int cnb_ctx_destroy(cnb_ctx *c) {
     cudaFree(c->tile_hist);
     cudaFree(c->sweep);
     cudaFree(c->flags);
+    cudaFree(c->near);
+    cudaFree(c->sort_stats);
     cudaFree(c->group_scratch);
     delete c;
     return CNB_OK;
@@ -592,8 +622,28 @@ extern "C" int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *k
     if (!ctx || n < 0 || key_bits < 1 || key_bits > 64) return CNB_E_INVALID_ARG;
     if (n > ctx->n_max) return CNB_E_TOO_LARGE;
     if (n > 0 && (!keys_in || !keys_out || !perm_out)) return CNB_E_INVALID_ARG;
-    return cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, idx_in, perm_out, n, key_bits,
-                                    cnb::as_stream(stream));
+    cudaStream_t st = cnb::as_stream(stream);
+    const int32_t *skip = nullptr;
+    if (ctx->sort_mode == CNB_SORT_ADAPTIVE && n > 0 && idx_in == nullptr && keys_in != keys_out)
+        CNB_TRY(cnb::sort_pairs_near(ctx, keys_in, keys_out, perm_out, n, st, &skip));
+    return cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, idx_in, perm_out, n, key_bits, st,
+                                    skip);
+}
+
+extern "C" int cnb_ctx_set_sort_mode(cnb_ctx *ctx, int mode) {
+    if (!ctx || (mode != CNB_SORT_FULL && mode != CNB_SORT_ADAPTIVE)) return CNB_E_INVALID_ARG;
+    ctx->sort_mode = mode;
+    return CNB_OK;
+}
+
+extern "C" int cnb_ctx_sort_stats(cnb_ctx *ctx, int64_t *out) {
+    if (!ctx || !out) return CNB_E_INVALID_ARG;
+    unsigned long long v[2];
+    CNB_CUDA(cudaDeviceSynchronize());
+    CNB_CUDA(cudaMemcpy(v, ctx->sort_stats, sizeof(v), cudaMemcpyDeviceToHost));
+    out[0] = (int64_t)v[0];
+    out[1] = (int64_t)v[1];
+    return CNB_OK;
 }
 
 extern "C" int cnb_ctx_take_flags(cnb_ctx *ctx, int32_t *status, void *stream) {

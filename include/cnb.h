@@ -39,6 +39,7 @@ extern "C" {
 #define CNB_FLAG_NONFINITE 4      /* non-finite acceleration produced */
 #define CNB_FLAG_LIST_OVERFLOW 8  /* grouped traversal work queue exhausted */
 #define CNB_FLAG_WAIT_LIMIT 16    /* a bounded wait between blocks gave up (result invalid) */
+#define CNB_FLAG_SORT_CHECK 32    /* a destination check of the near-sorted path failed (result invalid) */
 
 /* Morton key modes */
 #define CNB_KEY_COMPAT30 0 /* bit-exact with morton.py:13-63 (low 10 bits of each 21-bit coordinate) */
@@ -85,6 +86,27 @@ int cnb_ctx_destroy(cnb_ctx *ctx);
 int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                    const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
                    void *stream);
+
+/* No counterpart in the reference.  Sort mode of a context (default
+ * CNB_SORT_FULL).  CNB_SORT_ADAPTIVE: cnb_sort_pairs with idx_in == NULL and
+ * keys_in != keys_out first tries the near-sorted path -- keys that break
+ * the ascending order (at every descent the shorter of the out-of-order runs
+ * on its two sides, repeated in 4096-key windows until what is left ascends)
+ * and keys outside the running max / min of the rest are taken out, sorted,
+ * and merged back -- and runs the
+ * full radix sort only when more than CNB_SORT_NEAR_CAP keys had to be
+ * taken out.  Both paths return the same stable argsort; the choice is made
+ * on the device (no synchronisation, capturable in a CUDA graph).  Bodies
+ * that were sorted by their keys one step earlier mostly keep their order. */
+#define CNB_SORT_FULL 0
+#define CNB_SORT_ADAPTIVE 1
+#define CNB_SORT_NEAR_CAP 2048
+int cnb_ctx_set_sort_mode(cnb_ctx *ctx, int mode);
+
+/* No counterpart in the reference.  out[0] = sorts of this context that took
+ * the near-sorted path, out[1] = sorts that ran the full radix sort (host
+ * array of 2; synchronises the device). */
+int cnb_ctx_sort_stats(cnb_ctx *ctx, int64_t *out);
 
 /* No counterpart in the reference: ORs the flags the context's kernels
  * raised into the caller's device status word and clears them (stream

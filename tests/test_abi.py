@@ -59,6 +59,8 @@ def test_host_only_entry_points():
                                     5, 0.5, 1, 8, 1.0, 0.01, 1.0, None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_sort_pairs(None, None, None, None, None, 5, 30, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_ctx_take_flags(None, None, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_ctx_set_sort_mode(None, _lib.SORT_ADAPTIVE) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_ctx_sort_stats(None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_render_density(None, None, None, None, None, 4, 0, 4, None) == _lib.CNB_E_INVALID_ARG
 
 
