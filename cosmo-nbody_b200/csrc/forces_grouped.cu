@@ -13,7 +13,10 @@
 // 32 entries, every lane applies them to its bodies: float32, rsqrt, and the
 // per-pair minimum image only for entries whose image can differ between the
 // bucket's bodies (flagged by a negative mass), so the force loop reads
-// shared memory only and never diverges.
+// shared memory only and never diverges.  The reference's cut (no force from a
+// node at d^2 <= 1e-7) is tested only on the second list's entries: those
+// with a per-pair image and those within sqrt(2e-7) of the bucket's box, the
+// only ones the cut can reach.
 //
 // Opening tests (bucket box B with centre g and half-size h, node CoM image c
 // nearest g, dmin = periodic distance from c to B, per axis):
@@ -146,10 +149,18 @@ __device__ __forceinline__ float image_of(float d) {
     return d > 0.5f ? 1.f : (d < -0.5f ? -1.f : 0.f);
 }
 
+// The reference's cut d^2 > 1e-7 can only drop a pair whose node lies within
+// sqrt(1e-7) of the bucket's box.  The walk sends every accepted entry whose
+// distance^2 to the box is at most kCutGuard (twice the cut: a margin far
+// above the rounding of the box distance) to the list applied WITH the cut;
+// the other entries are at d^2 > 1e-7 from every body of the bucket and skip
+// the test.
+constexpr float kCutGuard = 2e-7f;
+
 // Applies cnt list entries (x, y, z, mass) to the lane's BPL bodies.  WRAP:
 // the entries' image may differ between the bucket's bodies, so every pair
-// takes its own minimum image.
-template <int BPL, bool WRAP>
+// takes its own minimum image.  CUT: apply the reference's d^2 > 1e-7 cut.
+template <int BPL, bool WRAP, bool CUT>
 __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const float (&x)[BPL],
                                            const float (&y)[BPL], const float (&z)[BPL],
                                            float soft2, float (&ax)[BPL], float (&ay)[BPL],
@@ -170,7 +181,7 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
             }
             const float q = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
             const float r = rsqrtf(q);
-            const float f = (q > cut) ? e.w * r * r * r : 0.f;
+            const float f = (!CUT || q > cut) ? e.w * r * r * r : 0.f;
             ax[b] = fmaf(f, dx, ax[b]);
             ay[b] = fmaf(f, dy, ay[b]);
             az[b] = fmaf(f, dz, az[b]);
@@ -185,7 +196,7 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
 // are bit-identical to it; only the minimum image is formed differently
 // (d - rint(d) through the 1.5 * 2^23 rounding constant, equal to image_of on
 // |d| < 1.5).
-template <bool WRAP>
+template <bool WRAP, bool CUT>
 __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, const float (&x)[2],
                                                 const float (&y)[2], const float (&z)[2],
                                                 float soft2, float (&ax)[2], float (&ay)[2],
@@ -222,8 +233,10 @@ __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, con
         for (int u = 0; u < 8; ++u) {
             const float2 q = d2[u];
             float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
-            r0 = q.x > cut ? r0 : 0.f;
-            r1 = q.y > cut ? r1 : 0.f;
+            if (CUT) {
+                r0 = q.x > cut ? r0 : 0.f;
+                r1 = q.y > cut ? r1 : 0.f;
+            }
             const float2 r = make_float2(r0, r1);
             f[u] = __fmul2_rn(__fmul2_rn(__fmul2_rn(w[u], r), r), r);
         }
@@ -246,8 +259,10 @@ __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, con
         }
         const float2 q = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
         float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
-        r0 = q.x > cut ? r0 : 0.f;
-        r1 = q.y > cut ? r1 : 0.f;
+        if (CUT) {
+            r0 = q.x > cut ? r0 : 0.f;
+            r1 = q.y > cut ? r1 : 0.f;
+        }
         const float2 r = make_float2(r0, r1);
         const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(b.z, b.w), r), r), r);
         fx = __ffma2_rn(f, dx, fx);
@@ -272,15 +287,15 @@ __device__ __forceinline__ void put_entry(float4 *list, int idx, float4 e) {
     }
 }
 
-template <int BPL, bool WRAP>
+template <int BPL, bool WRAP, bool CUT>
 __device__ __forceinline__ void apply_entries(const float4 *list, int cnt, const float (&x)[BPL],
                                               const float (&y)[BPL], const float (&z)[BPL],
                                               float soft2, float (&ax)[BPL], float (&ay)[BPL],
                                               float (&az)[BPL]) {
     if constexpr (BPL == 2)
-        apply_list_pair<WRAP>(list, cnt, x, y, z, soft2, ax, ay, az);
+        apply_list_pair<WRAP, CUT>(list, cnt, x, y, z, soft2, ax, ay, az);
     else
-        apply_list<BPL, WRAP>(list, cnt, x, y, z, soft2, ax, ay, az);
+        apply_list<BPL, WRAP, CUT>(list, cnt, x, y, z, soft2, ax, ay, az);
 }
 
 // float4 slots per entry of the second list: the per-pair-image list, or
@@ -456,14 +471,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                     const int c = min(32, h.x - j0);
                     if (lane < c) put_entry<BPL>(list, lane, far[j0 + lane]);
                     __syncwarp();
-                    apply_entries<BPL, false>(list, c, x, y, z, soft2, ax, ay, az);
+                    apply_entries<BPL, false, false>(list, c, x, y, z, soft2, ax, ay, az);
                     __syncwarp();
                 }
                 for (int j0 = 0; j0 < h.y; j0 += 32) {
                     const int c = min(32, h.y - j0);
                     if (lane < c) put_entry<BPL>(list, lane, far[P.far_cap - h.y + j0 + lane]);
                     __syncwarp();
-                    apply_entries<BPL, true>(list, c, x, y, z, soft2, ax, ay, az);
+                    apply_entries<BPL, true, true>(list, c, x, y, z, soft2, ax, ay, az);
                     __syncwarp();
                 }
                 n_entries += h.x + h.y;
@@ -494,7 +509,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                 set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
                 node = -1;
             }
-            bool accept = false, open = false, consistent = true;
+            bool accept = false, open = false, consistent = true, near_box = false;
             float4 E = make_float4(0.f, 0.f, 0.f, 0.f);
             int32_t c0 = -1, c1 = -1;
             if (node >= 0) {
@@ -509,13 +524,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                     dx -= sx_;
                     dy -= sy_;
                     dz -= sz_;
+                    const float tx = fmaxf(fabsf(dx) - ghx, 0.f);
+                    const float ty = fmaxf(fabsf(dy) - ghy, 0.f);
+                    const float tz = fmaxf(fabsf(dz) - ghz, 0.f);
+                    const float d2min = tx * tx + ty * ty + tz * tz;
+                    near_box = d2min <= kCutGuard;
                     if (c0 == -1) {
                         accept = true;
                     } else {
-                        const float tx = fmaxf(fabsf(dx) - ghx, 0.f);
-                        const float ty = fmaxf(fabsf(dy) - ghy, 0.f);
-                        const float tz = fmaxf(fabsf(dz) - ghz, 0.f);
-                        const float d2min = tx * tx + ty * ty + tz * tz;
                         if (EWALD) {
                             // periodic law: every image is valid; the node's size is its
                             // 3-D extent, or b_max when quadrupoles are applied
@@ -561,7 +577,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             const uint32_t am = __ballot_sync(0xffffffffu, accept);
             const uint32_t om = __ballot_sync(0xffffffffu, open);
             // second list: per-pair image, or (periodic law) an internal node's quadrupole
-            const bool to_w = EWALD ? (accept && P.quad != nullptr && c0 != -1) : (accept && E.w < 0.f);
+            // (reference law: also every entry near enough to the box for the cut to apply)
+            const bool to_w = EWALD ? (accept && P.quad != nullptr && c0 != -1)
+                                    : (accept && (E.w < 0.f || near_box));
             const uint32_t wm = __ballot_sync(0xffffffffu, to_w);
             const uint32_t nm = am & ~wm;
             if (accept) {
@@ -579,7 +597,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                         eg[1] += pq[1];
                         eg[2] += pq[2];
                     } else {
-                        put_entry<BPL>(wlist, w, make_float4(E.x, E.y, E.z, -E.w));
+                        put_entry<BPL>(wlist, w, make_float4(E.x, E.y, E.z, fabsf(E.w)));
                     }
                 } else {
                     put_entry<BPL>(list, cnt + __popc(nm & lt), E);
@@ -601,7 +619,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             }
             __syncwarp();
             if (cnt >= 32) {
-                apply_entries<BPL, false>(list, 32, x, y, z, soft2, ax, ay, az);
+                apply_entries<BPL, false, EWALD>(list, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 __syncwarp();
 #pragma unroll
@@ -614,7 +632,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                 if (EWALD)
                     apply_quad<BPL>(wlist, 32, x, y, z, soft2, ax, ay, az);
                 else
-                    apply_entries<BPL, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
+                    apply_entries<BPL, true, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 n_wrap += 32;
                 __syncwarp();
@@ -625,11 +643,11 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                 __syncwarp();
             }
         }
-        apply_entries<BPL, false>(list, cnt, x, y, z, soft2, ax, ay, az);
+        apply_entries<BPL, false, EWALD>(list, cnt, x, y, z, soft2, ax, ay, az);
         if (EWALD)
             apply_quad<BPL>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
         else
-            apply_entries<BPL, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
+            apply_entries<BPL, true, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
         n_entries += cnt + wcnt;
         n_wrap += wcnt;
         __syncwarp();
@@ -775,14 +793,18 @@ __global__ void __launch_bounds__(kSWarps * 32) k_super_lists(SuperParams P) {
                     dy -= sy_;
                     dz -= sz_;
                     const float adx = fabsf(dx), ady = fabsf(dy), adz = fabsf(dz);
-                    const int far_cls = (adx < wlx && ady < wly && adz < wlz) ? 1 : 2;
+                    const float tx = fmaxf(adx - hx, 0.f), ty = fmaxf(ady - hy, 0.f),
+                                tz = fmaxf(adz - hz, 0.f);
+                    const float d2min = tx * tx + ty * ty + tz * tz;
+                    // the per-pair part also takes every entry near enough to
+                    // the box for the reference's cut to apply (it is applied with it)
+                    const int far_cls =
+                        (adx < wlx && ady < wly && adz < wlz && d2min > kCutGuard) ? 1 : 2;
                     if (c0 == -1) {
                         cls = far_cls;
                     } else {
                         const float s = S.x > P.half_box ? P.box : S.x;
-                        const float tx = fmaxf(adx - hx, 0.f), ty = fmaxf(ady - hy, 0.f),
-                                    tz = fmaxf(adz - hz, 0.f);
-                        if (s * s < P.th2 * (tx * tx + ty * ty + tz * tz)) {
+                        if (s * s < P.th2 * d2min) {
                             cls = far_cls;
                         } else {
                             const float ux = fminf(adx + hx, P.half_box),

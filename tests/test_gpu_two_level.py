@@ -33,6 +33,21 @@ def _bodies(kind, n_grid, seed):
         bg = rng.random(n) < 0.3
         p[bg] = rng.random((int(bg.sum()), 3))
         x, y, z = (np.mod(p[:, i], 1.0).astype(np.float32) for i in range(3))
+    elif kind == "close_pairs":
+        # companions planted next to 90 bodies at distances on both sides of
+        # the reference's cut d^2 > 1e-7 (sqrt = 3.16e-4), one coincident
+        (x, y, z), _ = zeldovich_arrays(n_grid, seed)
+        x, y, z = (np.array(a, np.float64) for a in (x, y, z))
+        rng = np.random.default_rng(seed + 7)
+        n = x.size
+        idx = rng.choice(np.arange(0, n - 1, 2), 90, replace=False)
+        dist = np.array([0.0, 1e-4, 2.5e-4, 3.0e-4, 3.4e-4, 4e-4, 1e-3])
+        for k, i in enumerate(idx):
+            u = rng.normal(size=3)
+            u /= np.linalg.norm(u)
+            d = dist[k % dist.size] * u
+            x[i + 1], y[i + 1], z[i + 1] = x[i] + d[0], y[i] + d[1], z[i] + d[2]
+        x, y, z = (np.mod(a, 1.0).astype(np.float32) for a in (x, y, z))
     else:
         raise ValueError(kind)
     codes, _ = orc.compute_codes(x, y, z, 1)
@@ -41,7 +56,7 @@ def _bodies(kind, n_grid, seed):
 
 
 class Case:
-    def __init__(self, kind, n_grid, seed=0, bpl=1):
+    def __init__(self, kind, n_grid, seed=0, bpl=1, soft=None):
         from cnb.core.octree import OctreeManager
         pos, codes = _bodies(kind, n_grid, seed)
         self.pos_h = pos
@@ -51,7 +66,7 @@ class Case:
         self.bpl = bpl
         self.tm = OctreeManager(n, node_table=True, bucket=32 * bpl)
         self.tm.build(self.P, self.M, torch.from_numpy(codes).cuda())
-        self.soft = 0.5 / n_grid
+        self.soft = 0.5 / n_grid if soft is None else soft
         self.st = int(torch.cuda.current_stream().cuda_stream)
 
     def single(self, theta, warps=4):
@@ -123,6 +138,25 @@ def test_theta_zero_is_direct_sum():
     assert int(s2[0]) == c.n * c.n
     d = orc.direct_sum(*c.pos_h, np.full(c.n, 1.0 / c.n, np.float32), np.arange(c.n), 1.0, c.soft)
     _close(f2, d, 1e-4)
+
+
+@pytest.mark.parametrize("bpl", [1, 2])
+def test_cut_close_pairs(bpl):
+    """The reference's cut (no force from a node at d^2 <= 1e-7): with a small
+    softening the planted pairs inside the cut would dominate the force if
+    they were applied, and those just outside it must be.  Both traversals at
+    theta -> 0 (every entry a leaf) are the direct sum with the cut; at
+    theta = 0.5 they accept the same nodes and agree."""
+    c = Case("close_pairs", 16, 2, bpl, soft=1e-4)
+    m = np.full(c.n, 1.0 / c.n, np.float32)
+    d = orc.direct_sum(*c.pos_h, m, np.arange(c.n), 1.0, c.soft)
+    f1, _ = c.single(1e-6)
+    f2, _, hdr = c.two_level(1e-6, 64)
+    _close(f1, d, 1e-4)
+    _close(f2, d, 1e-4)
+    f1, _ = c.single(0.5)
+    f2, _, _ = c.two_level(0.5, 512)
+    _close(f2, f1)
 
 
 def test_overflowing_lists_fall_back_to_root_walk():
