@@ -142,10 +142,14 @@ __device__ __forceinline__ void ewald_quad(const float4 *__restrict__ T, int nt,
     out[2] = 0.5f * (xxz * mxx + yyz * myy + zzz * mzz) + xyz * mxy + xzz * mxz + yzz * myz;
 }
 
-// Nearest-image offset of a coordinate difference d with |d| < 1.5:
-// -1, 0 or +1, equal to rint(d) there (ties at +-0.5 round to 0, as rint
-// does); compare-and-select keeps it on the FP32 pipe.
-__device__ __forceinline__ float image_of(float d) {
+// Nearest-image offset of a coordinate difference d with |d| < 1.5: -1, 0
+// or +1 (ties at +-0.5 round to 0), i.e. rint(d) -- one instruction where a
+// compare-and-select chain takes four per axis.
+__device__ __forceinline__ float image_of(float d) { return rintf(d); }
+
+// The same offset by compare-and-select, on the FP32 / ALU pipes: the per-pair
+// form of the force loop, where rint on the XU pipe would compete with rsqrt.
+__device__ __forceinline__ float pair_image(float d) {
     return d > 0.5f ? 1.f : (d < -0.5f ? -1.f : 0.f);
 }
 
@@ -175,9 +179,9 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
         for (int b = 0; b < BPL; ++b) {
             float dx = e.x - x[b], dy = e.y - y[b], dz = e.z - z[b];
             if (WRAP) {
-                dx -= image_of(dx);
-                dy -= image_of(dy);
-                dz -= image_of(dz);
+                dx -= pair_image(dx);
+                dy -= pair_image(dy);
+                dz -= pair_image(dz);
             }
             const float q = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
             const float r = rsqrtf(q);
@@ -194,8 +198,8 @@ __device__ __forceinline__ void apply_list(const float4 *list, int cnt, const fl
 // operands and each FP32 instruction (FADD2 / FMUL2 / FFMA2, sm_100) serves
 // both.  The arithmetic, and its order, is the scalar loop's, so the forces
 // are bit-identical to it; only the minimum image is formed differently
-// (d - rint(d) through the 1.5 * 2^23 rounding constant, equal to image_of on
-// |d| < 1.5).
+// (d - rint(d) through the 1.5 * 2^23 rounding constant, equal to pair_image
+// on |d| < 1.5).
 template <bool WRAP, bool CUT>
 __device__ __forceinline__ void apply_list_pair(const float4 *list, int cnt, const float (&x)[2],
                                                 const float (&y)[2], const float (&z)[2],
