@@ -187,9 +187,21 @@ __device__ void mark_window(const uint64_t *__restrict__ keys, int64_t n, int64_
         *s_max = 0ull;
         *s_min = ~0ull;
     }
-    for (int j = threadIdx.x; j < wn; j += kNearThreads) {
-        sk[j] = __ldg(keys + lo + j);
-        mk[j] = 0;
+    {
+        uint64_t v[kNearWinItems];
+#pragma unroll
+        for (int q = 0; q < kNearWinItems; ++q) {
+            const int j = threadIdx.x + q * kNearThreads;
+            v[q] = j < wn ? __ldg(keys + lo + j) : 0ull;
+        }
+#pragma unroll
+        for (int q = 0; q < kNearWinItems; ++q) {
+            const int j = threadIdx.x + q * kNearThreads;
+            if (j < wn) {
+                sk[j] = v[q];
+                mk[j] = 0;
+            }
+        }
     }
     __syncthreads();
     int desc = 0;
@@ -225,10 +237,17 @@ __device__ void mark_window(const uint64_t *__restrict__ keys, int64_t n, int64_
             if (a > b) {
                 // the keys after the descent that are below a, and the keys
                 // before it that are above b: the shorter side is the one out
-                // of place (a displaced key or clump); ties mark the later side
+                // of place (a displaced key or clump); ties mark the later side.
+                // Both runs grow in step until one ends, so the scan stops
+                // at the shorter one.
                 int kf = 1, kb = 1;
-                while (kf < kNearReach && c + 1 + kf < U && sk[ci[c + 1 + kf]] < a) ++kf;
-                while (kb < kNearReach && c - kb >= 0 && sk[ci[c - kb]] > b) ++kb;
+                for (;;) {
+                    const bool f = kf < kNearReach && c + 1 + kf < U && sk[ci[c + 1 + kf]] < a;
+                    const bool g = kb < kNearReach && c - kb >= 0 && sk[ci[c - kb]] > b;
+                    kf += f;
+                    kb += g;
+                    if (!f || !g) break;
+                }
                 if (kf <= kb) {
                     for (int q = 1; q <= kf; ++q) mk[ci[c + q]] = 1;
                 } else {
