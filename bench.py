@@ -468,8 +468,12 @@ def accuracy(eng, args):
 def e2e(eng, args, ws):
     """The same step through the public API with host buffers: every step
     copies positions and velocities in from pinned host memory and copies
-    positions, velocities and the density grid back."""
+    positions, velocities and the density grid back.  `value`: the host-fed
+    stepping API (cnb.core.hoststep.HostStepper), whose copies run on their own
+    streams under the compute; `serial`: copy in, step, copy out one after
+    another on one stream."""
     import torch
+    from cnb.core.hoststep import HostStepper
     s = eng.state
     n = s.n
     host_in = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(6)]
@@ -478,8 +482,22 @@ def e2e(eng, args, ws):
     host_out = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(6)]
     grid_h = torch.empty(tuple(eng.camera.grid_d.shape), dtype=torch.float32, pin_memory=True)
     steps = args.steps
-    torch.cuda.synchronize()
+    main = torch.cuda.current_stream()
+    hs = HostStepper(eng)
+    for _ in range(2):
+        hs.submit(host_in, host_out, grid_h)
+    hs.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    hs.h2d.wait_stream(main)          # the first copy-in starts inside the timed region
+    for k in range(steps):
+        hs.submit(host_in, host_out, grid_h)
+    main.wait_stream(hs.d2h)          # ... and the last copy-out ends inside it
+    e1.record()
+    e1.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    # the same transfers one after another
+    torch.cuda.synchronize()
     e0.record()
     for k in range(steps):
         for h, d in zip(host_in, s.pos + s.vel):
@@ -491,10 +509,13 @@ def e2e(eng, args, ws):
         grid_h.copy_(eng.camera.grid_d, non_blocking=True)
     e1.record()
     e1.synchronize()
-    ms = max_over_ranks(e0.elapsed_time(e1), ws)
+    ms_serial = max_over_ranks(e0.elapsed_time(e1), ws)
     return {"value": ws * n * steps / (ms * 1e-3), "unit": "particle-steps/s",
             "h2d_bytes_per_step": 24 * n, "d2h_bytes_per_step": 24 * n + 4 * grid_h.numel(),
-            "api": "cnb.core.engine.SimulationEngine.step + Camera.splat (libcnb C ABI)"}
+            "api": "cnb.core.hoststep.HostStepper.submit (SimulationEngine.step + Camera.splat, "
+                   "copies on their own streams, two staging slots)",
+            "serial": {"value": ws * n * steps / (ms_serial * 1e-3),
+                       "api": "copy in, SimulationEngine.step + Camera.splat, copy out on one stream"}}
 
 
 def cpu_baseline(args):

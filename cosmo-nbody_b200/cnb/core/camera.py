@@ -27,13 +27,23 @@ class Camera:
         self.grid_d = torch.zeros((self.height, self.width), dtype=torch.float32, device=dev)
         self.box_center = (config.BOX_SIZE / 2, config.BOX_SIZE / 2, config.BOX_SIZE / 2)
         self.mvp_d = torch.zeros((4, 4), dtype=torch.float32, device=dev)
+        # pinned staging for the per-step MVP upload: a copy from pageable memory
+        # would stall the host until the stream drains
+        self._mvp_pin = [torch.empty((4, 4), dtype=torch.float32).pin_memory() for _ in range(4)]
+        self._mvp_ev = [torch.cuda.Event() for _ in range(4)]
+        self._mvp_i = 0
 
     def splat(self, step, px_d, py_d, pz_d):
         """camera.py:40-44: clear, MVP, render_density.  Returns the grid."""
         self.grid_d.zero_()
         mvp = get_mvp_matrix(step, self.box_center, self.config.BOX_SIZE, self.config,
                              aspect=self.width / self.height)
-        self.mvp_d.copy_(torch.from_numpy(mvp), non_blocking=False)
+        i = self._mvp_i
+        self._mvp_i = (i + 1) % len(self._mvp_pin)
+        self._mvp_ev[i].synchronize()          # the upload that last used this buffer has run
+        self._mvp_pin[i].copy_(torch.from_numpy(mvp))
+        self.mvp_d.copy_(self._mvp_pin[i], non_blocking=True)
+        self._mvp_ev[i].record()
         st = int(torch.cuda.current_stream(self.device).cuda_stream)
         _lib.call("cnb_render_density", px_d.data_ptr(), py_d.data_ptr(), pz_d.data_ptr(),
                   self.grid_d.data_ptr(), self.mvp_d.data_ptr(), px_d.shape[0], self.width,
