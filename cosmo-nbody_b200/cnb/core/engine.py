@@ -208,7 +208,8 @@ class SimulationEngine:
                 self.camera.colorize(out=frame)
 
     def capture(self, splat=True, colorize=False, step0=0):
-        """Capture two consecutive steps (and their splats) in one CUDA graph.
+        """Capture two consecutive steps (and their splats) in one CUDA graph;
+        each splat overlaps the step after it.
         The step alternates between two array sets, so after every replay the
         arrays are back where they were captured.  The two steps that run
         eagerly first (steps step0, step0 + 1 of the camera orbit) warm up
@@ -227,10 +228,23 @@ class SimulationEngine:
                 self.frame_slots = torch.empty((2, self.camera.height, self.camera.width, 3),
                                                dtype=torch.float32, device=dev)
 
+        side = torch.cuda.Stream(dev)
+
         def two_steps():
+            main = torch.cuda.current_stream(dev)
             for k in range(2):
-                self._step_device(self.mvp_slots[k] if self._graph_splat else None,
-                                  self.frame_slots[k] if self.frame_slots is not None else None)
+                self._step_device()
+                if self._graph_splat:
+                    # the splat reads only this step's positions, which the next
+                    # step's sort gathers from but does not overwrite: it runs
+                    # on a second stream beside that step
+                    side.wait_stream(main)
+                    with torch.cuda.stream(side):
+                        self.camera.splat_device(self.mvp_slots[k], *self.state.pos)
+                        if self.frame_slots is not None:
+                            self.camera.colorize(out=self.frame_slots[k])
+            if self._graph_splat:
+                main.wait_stream(side)
 
         two_steps()                      # warm-up, eager
         self.a += 2 * self.da
