@@ -41,10 +41,11 @@ sys.path.insert(0, os.path.join(ROOT, "cosmo-nbody_b200"))
 METRIC = "particle-steps/s at N=128^3 (full plain step + 1920x1080 splat)"
 N_GRID = 128
 FLOPS_PER_INTERACTION = 20   # 3 sub, 3 min-image, 5 d2, 1 +eps2, 1 rsqrt, 3 mul, 3 fma (+1)
+FULL_SORT_KERNELS = 10     # zeroing + digit histogram + 8 one-sweep passes (63-bit keys)
 # DRAM traffic of one k_forces_grouped launch on this workload (64-body buckets, two-level
 # walk), from the ncu capture summarised in profiles/k_forces_grouped_128cube.md
 # (dram__bytes_read.sum + dram__bytes_write.sum)
-FORCES_TRAFFIC_BYTES_128 = 219.6e6 + 21.7e6
+FORCES_TRAFFIC_BYTES_128 = 213.2e6 + 21.8e6
 
 
 def parse():
@@ -354,6 +355,7 @@ def run_ours(args):
         while time.time() < t_end:
             eng.replay() if args.graph else one_step(step0)
             torch.cuda.synchronize()
+    near0 = state._ctx.stats()[0]
     barrier(ws)
     launches0 = _lib.launch_count()
     # graph mode: one replay = two steps; an odd K ends with one eager device step
@@ -383,14 +385,18 @@ def run_ours(args):
     eng.check()
     value = aggregate_rate(n, steps_done, ws, total_ms)
     args.steps_done = steps_done
-    launches = launches_per_step
+    launches = launches_per_step * steps_done
+    if args.graph:
+        # a captured sort holds the full radix sort (zeroing, histogram, 8 passes) in a
+        # conditional node that does not run when the near-sorted path took the sort
+        launches -= FULL_SORT_KERNELS * (state._ctx.stats()[0] - near0)
 
     line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws,
             "steps": steps_done, "warmup": args.warmup, "ms_per_step": total_ms / steps_done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Zel'dovich ICs)", "config": config_dict(cfg, args),
-            "gpu_launches": int(launches) * steps_done,
-            "gpu_launches_per_step": int(launches), "cuda_graph": bool(args.graph),
+            "gpu_launches": int(launches),
+            "gpu_launches_per_step": round(launches / steps_done, 1), "cuda_graph": bool(args.graph),
             "stages_ms_eager": stages}
     if tune_report is not None:
         line["autotune"] = tune_report

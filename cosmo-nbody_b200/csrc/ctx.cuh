@@ -19,6 +19,7 @@ struct cnb_ctx {
     int sort_mode = CNB_SORT_FULL;
     void *near = nullptr;
     unsigned long long *sort_stats = nullptr;  // [near-sorted path taken, full radix sorts run]
+    cudaStream_t side = nullptr;    // captures the full sort into a conditional graph node
     // grouped traversal scratch (grown on demand by cnb_forces_grouped)
     void *group_scratch = nullptr;
     size_t group_scratch_bytes = 0;
@@ -32,7 +33,8 @@ constexpr int kNearTile = kNearThreads * kNearItems;  // 4096 keys
 constexpr int kNearCap = 2048;                        // at most this many keys leave their run
 int64_t near_bytes(int64_t n_max);
 int sort_pairs_near(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
-                    uint32_t *perm_out, int64_t n, cudaStream_t st, const int32_t **skip_full);
+                    uint32_t *perm_out, int64_t n, cudaStream_t st, const int32_t **skip_full,
+                    const int32_t **never, cudaGraphConditionalHandle cond, bool use_cond);
 int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                         const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
                         cudaStream_t st, const int32_t *skip = nullptr);

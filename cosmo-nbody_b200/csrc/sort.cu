@@ -611,6 +611,7 @@ extern "C" int cnb_ctx_destroy(cnb_ctx *c) {
     cudaFree(c->flags);
     cudaFree(c->near);
     cudaFree(c->sort_stats);
+    if (c->side) cudaStreamDestroy(c->side);
     cudaFree(c->group_scratch);
     delete c;
     return CNB_OK;
@@ -623,11 +624,50 @@ extern "C" int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *k
     if (n > ctx->n_max) return CNB_E_TOO_LARGE;
     if (n > 0 && (!keys_in || !keys_out || !perm_out)) return CNB_E_INVALID_ARG;
     cudaStream_t st = cnb::as_stream(stream);
-    const int32_t *skip = nullptr;
-    if (ctx->sort_mode == CNB_SORT_ADAPTIVE && n > 0 && idx_in == nullptr && keys_in != keys_out)
-        CNB_TRY(cnb::sort_pairs_near(ctx, keys_in, keys_out, perm_out, n, st, &skip));
-    return cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, idx_in, perm_out, n, key_bits, st,
-                                    skip);
+    const int32_t *skip = nullptr, *never = nullptr;
+    if (!(ctx->sort_mode == CNB_SORT_ADAPTIVE && n > 0 && idx_in == nullptr && keys_in != keys_out))
+        return cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, idx_in, perm_out, n, key_bits, st);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CNB_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusActive) {
+        // eager: the full sort's kernels follow and return at once when the
+        // near-sorted path produced the result
+        CNB_TRY(cnb::sort_pairs_near(ctx, keys_in, keys_out, perm_out, n, st, &skip, &never, 0,
+                                     false));
+        return cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, nullptr, perm_out, n, key_bits,
+                                        st, skip);
+    }
+    // captured: the full sort goes into the body of a conditional node that
+    // runs unless the near-sorted path clears it (default 1 at every launch)
+    cudaGraph_t g = nullptr;
+    CNB_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, nullptr, nullptr));
+    cudaGraphConditionalHandle cond;
+    CNB_CUDA(cudaGraphConditionalHandleCreate(&cond, g, 1u, cudaGraphCondAssignDefault));
+    CNB_TRY(cnb::sort_pairs_near(ctx, keys_in, keys_out, perm_out, n, st, &skip, &never, cond,
+                                 true));
+    const cudaGraphNode_t *deps = nullptr;
+    size_t nd = 0;
+    CNB_CUDA(cudaStreamGetCaptureInfo(st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams p = {};
+    p.type = cudaGraphNodeTypeConditional;
+    p.conditional.handle = cond;
+    p.conditional.type = cudaGraphCondTypeIf;
+    p.conditional.size = 1;
+    cudaGraphNode_t node;
+    CNB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+    cudaGraph_t body = p.conditional.phGraph_out[0];
+    if (!ctx->side) CNB_CUDA(cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking));
+    CNB_CUDA(cudaStreamBeginCaptureToGraph(ctx->side, body, nullptr, nullptr, 0,
+                                           cudaStreamCaptureModeRelaxed));
+    // `never` keeps the body's zeroing a kernel (the flag it reads stays 0)
+    const int rc = cnb::sort_pairs_onesweep(ctx, keys_in, keys_out, nullptr, perm_out, n, key_bits,
+                                            ctx->side, never);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->side, &captured);
+    CNB_TRY(rc);
+    CNB_CUDA(e);
+    CNB_CUDA(cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return CNB_OK;
 }
 
 extern "C" int cnb_ctx_set_sort_mode(cnb_ctx *ctx, int mode) {

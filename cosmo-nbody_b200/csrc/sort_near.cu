@@ -365,7 +365,9 @@ __global__ void __launch_bounds__(kNearThreads) k_near_mark(const uint64_t *__re
 
 __global__ void __launch_bounds__(kNearThreads) k_near_filter(const uint64_t *__restrict__ keys,
                                                               int64_t n, int64_t nt, NearWs w,
-                                                              unsigned long long *stats) {
+                                                              unsigned long long *stats,
+                                                              cudaGraphConditionalHandle cond,
+                                                              bool use_cond) {
     __shared__ uint64_t wtot[kNearThreads / 32];
     __shared__ uint32_t wsum[kNearThreads / 32];
     __shared__ int s_first, s_last;
@@ -463,6 +465,8 @@ __global__ void __launch_bounds__(kNearThreads) k_near_filter(const uint64_t *__
         if (run <= (uint32_t)kNearCap) {
             w.ctl[1] = 1;
             if (stats) stats[0] += 1ull;
+            // in a CUDA graph: the full sort's conditional node (default: run) is skipped
+            if (use_cond) cudaGraphSetConditional(cond, 0u);
         }
     }
 }
@@ -649,9 +653,13 @@ int64_t near_bytes(int64_t n_max) {
 }
 
 // Launches the near-sorted path; *skip_full receives the device flag that
-// is non-zero when it produced the result (the full sort's kernels then return).
+// is non-zero when it produced the result (the full sort's kernels then
+// return), *never a device flag that stays zero.  use_cond: the launches are
+// being captured into a CUDA graph whose conditional node `cond` holds the
+// full sort; the path sets it to 0 when it produced the result.
 int sort_pairs_near(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
-                    uint32_t *perm_out, int64_t n, cudaStream_t st, const int32_t **skip_full) {
+                    uint32_t *perm_out, int64_t n, cudaStream_t st, const int32_t **skip_full,
+                    const int32_t **never, cudaGraphConditionalHandle cond, bool use_cond) {
     const int64_t nt = (n + kNearTile - 1) / kNearTile;
     const int64_t nt_max = (ctx->n_max + kNearTile - 1) / kNearTile;
     NearWs w;
@@ -663,7 +671,8 @@ int sort_pairs_near(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                                   (int)kNearPlaceSmem));
     k_near_mark<<<(unsigned)nt, kNearThreads, kNearMarkSmem, st>>>(keys_in, n, nt, w);
     CNB_TRY(launch_status());
-    k_near_filter<<<(unsigned)nt, kNearThreads, 0, st>>>(keys_in, n, nt, w, ctx->sort_stats);
+    k_near_filter<<<(unsigned)nt, kNearThreads, 0, st>>>(keys_in, n, nt, w, ctx->sort_stats, cond,
+                                                          use_cond);
     CNB_TRY(launch_status());
     k_near_take<<<(unsigned)nt, kNearThreads, 0, st>>>(keys_in, nt, w);
     CNB_TRY(launch_status());
@@ -671,6 +680,7 @@ int sort_pairs_near(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                                                                       perm_out, ctx->flags);
     CNB_TRY(launch_status());
     *skip_full = w.ctl + 1;
+    *never = w.ctl + 7;  // zeroed with the rest of ctl, never set
     return CNB_OK;
 }
 

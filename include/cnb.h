@@ -96,8 +96,10 @@ int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
  * and merged back -- and runs the
  * full radix sort only when more than CNB_SORT_NEAR_CAP keys had to be
  * taken out.  Both paths return the same stable argsort; the choice is made
- * on the device (no synchronisation, capturable in a CUDA graph).  Bodies
- * that were sorted by their keys one step earlier mostly keep their order. */
+ * on the device (no synchronisation).  When the stream is being captured into
+ * a CUDA graph, the full sort goes into a conditional node that the
+ * near-sorted path switches off when it produced the result.  Bodies that
+ * were sorted by their keys one step earlier mostly keep their order. */
 #define CNB_SORT_FULL 0
 #define CNB_SORT_ADAPTIVE 1
 #define CNB_SORT_NEAR_CAP 2048

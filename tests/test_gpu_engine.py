@@ -306,8 +306,9 @@ def test_run_replays_graph_with_frames(n_steps):
     assert len(frames_g) == n_steps
     for a, b in zip(eager.state.pos + eager.state.vel, graphed.state.pos + graphed.state.vel):
         np.testing.assert_array_equal(host(a), host(b))
+    # the splat sums with float atomics in arrival order: pixels differ in the last bits
     for fe, fg in zip(frames_e, frames_g):
-        np.testing.assert_allclose(host(fe), host(fg), rtol=1e-4, atol=1e-6)
+        np.testing.assert_allclose(host(fe), host(fg), rtol=1e-4, atol=1e-5)
     assert abs(graphed.a - eager.a) < 1e-12
     # and close to the host-scalar step of the reference's loop
     plain = SimulationEngine(cfg, SimulationState(16 ** 3, pos, vel))
