@@ -39,6 +39,11 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "cosmo-nbody_b200"))
 
 METRIC = "particle-steps/s at N=128^3 (full plain step + 1920x1080 splat)"
+
+
+def metric_for(n_grid):
+    """The metric string for an n_grid^3 run (METRIC for the default 128^3)."""
+    return METRIC.replace("N=128^3", f"N={n_grid}^3")
 N_GRID = 128
 FLOPS_PER_INTERACTION = 20   # 3 sub, 3 min-image, 5 d2, 1 +eps2, 1 rsqrt, 3 mul, 3 fma (+1)
 FULL_SORT_KERNELS = 10     # zeroing + digit histogram + 8 one-sweep passes (63-bit keys)
@@ -277,7 +282,7 @@ def run_reference(args):
         total += s
     value = n * args.steps / total
     line = {
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "impl": "reference", "metric": metric_for(args.n_grid), "value": value, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Zel'dovich ICs)",
@@ -392,7 +397,7 @@ def run_ours(args):
         # conditional node that does not run when the near-sorted path took the sort
         launches -= FULL_SORT_KERNELS * (state._ctx.stats()[0] - near0)
 
-    line = {"metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": ws,
+    line = {"metric": metric_for(args.n_grid), "value": value, "unit": "particle-steps/s", "n_gpus": ws,
             "steps": steps_done, "warmup": args.warmup, "ms_per_step": total_ms / steps_done,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Zel'dovich ICs)", "config": config_dict(cfg, args),
