@@ -38,7 +38,9 @@
 //                     accepted node, accumulated per lane while walking and
 //                     applied per body once per bucket (ewald.cu has the law).
 //                     With quadrupole moments the second list carries the
-//                     internal nodes with their second central moments.
+//                     internal nodes with their second central moments (and
+//                     the first list keeps the cut); without, the entries near
+//                     the bucket's box (the cut's).
 // theta is one value or one per bucket (learned controller).
 //
 // Two bodies per lane run the force loop on packed float2 (FADD2 / FMUL2 /
@@ -383,8 +385,12 @@ __device__ __forceinline__ void apply_quad(const float4 *q, int cnt, const float
     }
 }
 
-template <int BPL, int WARPS, bool EWALD>
+// LAW: 0 the minimum-image laws (CNB_MAC_REF_X, CNB_MAC_PERIODIC), 1 the
+// periodic (Ewald) law with monopoles, 2 the periodic law with quadrupoles.
+template <int BPL, int WARPS, int LAW>
 __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) {
+    constexpr bool EWALD = LAW != 0;
+    constexpr bool QUAD = LAW == 2;
     extern __shared__ __align__(16) unsigned char g_smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
@@ -580,16 +586,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             n_tests += (node >= 0);
             const uint32_t am = __ballot_sync(0xffffffffu, accept);
             const uint32_t om = __ballot_sync(0xffffffffu, open);
-            // second list: per-pair image, or (periodic law) an internal node's quadrupole
-            // (reference law: also every entry near enough to the box for the cut to apply)
-            const bool to_w = EWALD ? (accept && P.quad != nullptr && c0 != -1)
+            // second list: per-pair image, or (periodic law) an internal node's quadrupole;
+            // also every entry near enough to the box for the cut to apply, except with
+            // quadrupoles (the first list then keeps the cut)
+            const bool to_w = EWALD ? (accept && (QUAD ? c0 != -1 : near_box))
                                     : (accept && (E.w < 0.f || near_box));
             const uint32_t wm = __ballot_sync(0xffffffffu, to_w);
             const uint32_t nm = am & ~wm;
             if (accept) {
                 if (to_w) {
                     const int w = wcnt + __popc(wm & lt);
-                    if (EWALD) {
+                    if (EWALD && !QUAD) {
+                        put_entry<BPL>(wlist, w, E);  // near the box: a monopole with the cut
+                    } else if (EWALD) {
                         const float4 qa = __ldg(P.quad + 2 * node), qb = __ldg(P.quad + 2 * node + 1);
                         wlist[3 * w] = E;
                         wlist[3 * w + 1] = qa;
@@ -623,7 +632,10 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             }
             __syncwarp();
             if (cnt >= 32) {
-                apply_entries<BPL, false, EWALD>(list, 32, x, y, z, soft2, ax, ay, az);
+                if (QUAD)
+                    apply_entries<BPL, false, true>(list, 32, x, y, z, soft2, ax, ay, az);
+                else
+                    apply_entries<BPL, false, false>(list, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 __syncwarp();
 #pragma unroll
@@ -633,23 +645,32 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                 __syncwarp();
             }
             if (wcnt >= 32) {
-                if (EWALD)
+                if (QUAD)
                     apply_quad<BPL>(wlist, 32, x, y, z, soft2, ax, ay, az);
+                else if (EWALD)
+                    apply_entries<BPL, false, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
                 else
                     apply_entries<BPL, true, true>(wlist, 32, x, y, z, soft2, ax, ay, az);
                 n_entries += 32;
                 n_wrap += 32;
                 __syncwarp();
+                // float4 slots per entry: quadrupole entries, or the monopole layout
+                const int ww = (QUAD) ? SW : EW;
 #pragma unroll
                 for (int w = 0; w < SW; ++w)
-                    if (lane < wcnt - 32) wlist[SW * lane + w] = wlist[SW * (32 + lane) + w];
+                    if (w < ww && lane < wcnt - 32) wlist[ww * lane + w] = wlist[ww * (32 + lane) + w];
                 wcnt -= 32;
                 __syncwarp();
             }
         }
-        apply_entries<BPL, false, EWALD>(list, cnt, x, y, z, soft2, ax, ay, az);
-        if (EWALD)
+        if (QUAD)
+            apply_entries<BPL, false, true>(list, cnt, x, y, z, soft2, ax, ay, az);
+        else
+            apply_entries<BPL, false, false>(list, cnt, x, y, z, soft2, ax, ay, az);
+        if (QUAD)
             apply_quad<BPL>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
+        else if (EWALD)
+            apply_entries<BPL, false, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
         else
             apply_entries<BPL, true, true>(wlist, wcnt, x, y, z, soft2, ax, ay, az);
         n_entries += cnt + wcnt;
@@ -901,30 +922,35 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
     return launch_status();
 }
 
-template <int BPL, int WARPS, bool EWALD>
+template <int BPL, int WARPS, int LAW>
 static int launch_shape(GroupedParams &P, cudaStream_t st) {
-    const size_t smem = grouped_smem<BPL, EWALD>(WARPS);
-    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS, EWALD>,
+    const size_t smem = grouped_smem<BPL, LAW != 0>(WARPS);
+    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS, LAW>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS, EWALD>, WARPS * 32,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS, LAW>, WARPS * 32,
                                                   smem);
     // persistent grid: the work counter hands out buckets
-    k_forces_grouped<BPL, WARPS, EWALD><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
+    k_forces_grouped<BPL, WARPS, LAW><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
     return launch_status();
+}
+
+template <int BPL, int WARPS>
+static int launch_law(GroupedParams &P, cudaStream_t st) {
+    if (P.mac != CNB_MAC_EWALD) return launch_shape<BPL, WARPS, 0>(P, st);
+    return P.quad ? launch_shape<BPL, WARPS, 2>(P, st) : launch_shape<BPL, WARPS, 1>(P, st);
 }
 
 static int launch_grouped(GroupedParams &P, int bodies_per_lane, int block_warps,
                           cudaStream_t st) {
     CNB_CUDA(cudaMemsetAsync(P.ws + 1, 0, 2 * sizeof(int32_t), st));
-    const bool ew = (P.mac == CNB_MAC_EWALD);
     switch (bodies_per_lane * 16 + block_warps) {
-        case 16 + 2: return ew ? launch_shape<1, 2, true>(P, st) : launch_shape<1, 2, false>(P, st);
-        case 16 + 4: return ew ? launch_shape<1, 4, true>(P, st) : launch_shape<1, 4, false>(P, st);
-        case 16 + 8: return ew ? launch_shape<1, 8, true>(P, st) : launch_shape<1, 8, false>(P, st);
-        case 32 + 2: return ew ? launch_shape<2, 2, true>(P, st) : launch_shape<2, 2, false>(P, st);
-        case 32 + 4: return ew ? launch_shape<2, 4, true>(P, st) : launch_shape<2, 4, false>(P, st);
-        case 32 + 8: return ew ? launch_shape<2, 8, true>(P, st) : launch_shape<2, 8, false>(P, st);
+        case 16 + 2: return launch_law<1, 2>(P, st);
+        case 16 + 4: return launch_law<1, 4>(P, st);
+        case 16 + 8: return launch_law<1, 8>(P, st);
+        case 32 + 2: return launch_law<2, 2>(P, st);
+        case 32 + 4: return launch_law<2, 4>(P, st);
+        case 32 + 8: return launch_law<2, 8>(P, st);
         default: return CNB_E_INVALID_ARG;
     }
 }

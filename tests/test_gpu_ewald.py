@@ -100,13 +100,13 @@ def _sorted_bodies(n_grid, seed):
 
 
 class Tree:
-    def __init__(self, pos, codes, bpl=2):
+    def __init__(self, pos, codes, bpl=2, quad=False):
         from cnb.core.octree import OctreeManager
         self.n = n = codes.size
         self.P = [torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in pos]
         self.M = torch.full((n,), 1.0 / n, device="cuda")
         self.bpl = bpl
-        self.tm = OctreeManager(n, node_table=True, bucket=32 * bpl)
+        self.tm = OctreeManager(n, node_table=True, bucket=32 * bpl, quad=quad)
         self.tm.build(self.P, self.M, torch.from_numpy(codes).cuda())
         self.table = _table(64)
 
@@ -180,12 +180,52 @@ def test_theta_zero_matches_restated_bucket_algorithm():
     tr = Tree(pos, codes, bpl=1)
     soft = 0.5 / 8
     f, _ = tr.forces(0.0, soft)
+    want = _restated_theta_zero(tr, pos, soft)
+    scale = np.sqrt(np.mean(np.sum(want ** 2, 1)))
+    assert np.abs(f - want).max() < 2e-4 * scale, np.abs(f - want).max() / scale
+
+
+def _close_pair_bodies(n_grid, seed):
+    """Zel'dovich bodies with companions planted next to 40 of them at
+    distances on both sides of the reference's cut d^2 > 1e-7 (one coincident)."""
+    from cnb.utils.cosmology import zeldovich_arrays
+    (x, y, z), _ = zeldovich_arrays(n_grid, seed)
+    p = np.stack([x, y, z], 1).astype(np.float64)
+    rng = np.random.default_rng(seed + 11)
+    idx = rng.choice(np.arange(0, p.shape[0] - 1, 2), 40, replace=False)
+    dist = np.array([0.0, 1e-4, 2.5e-4, 3.0e-4, 3.4e-4, 4e-4, 1e-3])
+    for k, i in enumerate(idx):
+        u = rng.normal(size=3)
+        p[i + 1] = p[i] + dist[k % dist.size] * u / np.linalg.norm(u)
+    x, y, z = (np.mod(p[:, k], 1.0).astype(np.float32) for k in range(3))
+    codes, _ = orc.compute_codes(x, y, z, 1)
+    perm = orc.argsort_stable(codes)
+    return [a[perm] for a in (x, y, z)], codes[perm]
+
+
+@pytest.mark.parametrize("bpl,quad", [(1, False), (2, False), (2, True)])
+def test_theta_zero_close_pairs_honour_the_cut(bpl, quad):
+    """Without quadrupoles the cut is tested only on entries near each
+    bucket's box (the second list); with them, on the first list as a whole.
+    With softening 1e-4 a pair inside the cut would dominate the force
+    of its bodies if it were applied; the kernel must match the restatement,
+    which applies the cut to every pair."""
+    pos, codes = _close_pair_bodies(8, 3)
+    tr = Tree(pos, codes, bpl=bpl, quad=quad)
+    soft = 1e-4
+    f, _ = tr.forces(0.0, soft)
+    want = _restated_theta_zero(tr, pos, soft)
+    scale = np.sqrt(np.mean(np.sum(want ** 2, 1)))
+    assert np.abs(f - want).max() < 2e-4 * scale, np.abs(f - want).max() / scale
+
+
+def _restated_theta_zero(tr, pos, soft):
     T = tr.table.cpu().numpy().astype(np.float64)
     nt = 64
     p = np.stack(pos, 1).astype(np.float64)
     m = 1.0 / tr.n
     ws = tr.tm.workspace.cpu().numpy()
-    want = np.zeros_like(f)
+    want = np.zeros((tr.n, 3))
     for b in range(int(ws[0])):
         lo, cnt = ws[4 + 4 * b], ws[5 + 4 * b]
         body = p[lo:lo + cnt].astype(np.float32)
@@ -210,8 +250,7 @@ def test_theta_zero_matches_restated_bucket_algorithm():
             mono = d[keep] / (d2[keep] + soft * soft)[:, None] ** 1.5
             corr = -4 * math.pi / 3 * d + g + np.einsum("nij,j->ni", J, centre - p[i])
             want[i] = m * (mono.sum(0) + corr.sum(0))
-    scale = np.sqrt(np.mean(np.sum(want ** 2, 1)))
-    assert np.abs(f - want).max() < 2e-4 * scale, np.abs(f - want).max() / scale
+    return want
 
 
 def test_correction_error_falls_with_bucket_size():
@@ -351,8 +390,12 @@ def test_quadrupoles_lower_the_error():
           f"quadrupole: median {mq:.2e} p99 {pq:.2e} ({s_quad[0] / tm.n:.0f}/body)")
     # at the same theta: no worse than monopoles, with far fewer interactions
     assert mq < mm and pq < pm and s_quad[0] < 0.7 * s_mono[0], (mm, mq, pm, pq)
-    # theta = 0 accepts leaves only: no quadrupole entries, the same forces
+    # theta = 0 accepts leaves only: no quadrupole entries; the monopole mode's
+    # second list holds the leaves near each bucket's box (the cut's), which the
+    # quadrupole mode applies from its first list; the same forces up to rounding
     f0, s0 = tq.forces(0.0, soft)
-    g0, _ = tm.forces(0.0, soft)
-    assert int(s0[2]) == 0
-    np.testing.assert_array_equal(f0, g0)
+    g0, sg = tm.forces(0.0, soft)
+    assert int(s0[2]) == 0 and 0 < int(sg[2]) < int(sg[0])
+    scale = np.sqrt(np.mean(np.sum(g0 ** 2, 1)))
+    # float32 sums of 32 768 terms in two orders
+    assert np.abs(f0 - g0).max() < 1e-4 * scale
