@@ -1,0 +1,46 @@
+"""Host-side choices that need no GPU: which sort a configuration selects and
+how the benchmark names its metric."""
+import importlib.util
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_sort_mode_follows_the_key_mode():
+    from cnb.core.state import sort_mode_for
+    from cnb.utils import config as cfgmod
+    # auto: the near-sorted path for 63-bit keys, whose order survives a step;
+    # the full radix sort for the reference's 30-bit keys, whose low bits do not
+    assert sort_mode_for(cfgmod.make(SORT_MODE="auto"), "morton63") == "adaptive"
+    assert sort_mode_for(cfgmod.make(SORT_MODE="auto"), "compat30") == "full"
+    assert sort_mode_for(cfgmod.make(), "morton63") == "adaptive"   # the default is auto
+    for mode in ("full", "adaptive"):
+        for keys in ("morton63", "compat30"):
+            assert sort_mode_for(cfgmod.make(SORT_MODE=mode), keys) == mode
+    with pytest.raises(ValueError):
+        sort_mode_for(cfgmod.make(SORT_MODE="fast"), "morton63")
+
+
+def test_sort_mode_codes_match_the_header():
+    from cnb import _lib
+    from cnb.core.state import SORT_MODES
+    hdr = open(os.path.join(ROOT, "include", "cnb.h")).read()
+    assert f"#define CNB_SORT_FULL {SORT_MODES['full']}" in hdr
+    assert f"#define CNB_SORT_ADAPTIVE {SORT_MODES['adaptive']}" in hdr
+    assert f"#define CNB_SORT_NEAR_CAP {_lib.SORT_NEAR_CAP}" in hdr
+
+
+def test_bench_metric_names_the_grid_size():
+    spec = importlib.util.spec_from_file_location("bench_mod", os.path.join(ROOT, "bench.py"))
+    bench = importlib.util.module_from_spec(spec)
+    argv = sys.argv
+    try:
+        sys.argv = ["bench.py"]
+        spec.loader.exec_module(bench)
+    finally:
+        sys.argv = argv
+    assert bench.metric_for(128) == bench.METRIC          # the default run's metric is unchanged
+    assert "N=256^3" in bench.metric_for(256) and "128" not in bench.metric_for(256)
