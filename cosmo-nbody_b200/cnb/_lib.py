@@ -31,6 +31,7 @@ KEY_MORTON63 = 1
 MAC_REF_X = 0
 MAC_PERIODIC = 1
 MAC_EWALD = 2
+MAC_REF_X_BUCKET = 3
 SORT_FULL = 0
 SORT_ADAPTIVE = 1
 SORT_NEAR_CAP = 2048
@@ -83,7 +84,7 @@ SIGNATURES = {
                                   _d, _p, _p, _p]),
     "cnb_two_level_workspace_bytes": (_i64, [_i64, _int]),
     "cnb_forces_two_level": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _i64, _int, _p, _i64, _d, _int,
-                                    _int, _d, _d, _d, _p, _p, _p]),
+                                    _int, _int, _d, _d, _d, _p, _p, _p]),
     "cnb_make_buckets_boxes": (_int, [_p, _p, _p, _int, _i64, _int, _p, _p]),
     "cnb_compute_codes_boxes": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
     "cnb_box_roots": (_int, [_p, _p, _p, _int, _i64, _int, _p, _p]),

@@ -27,7 +27,8 @@ from .._arrays import check_status, status_buffer
 from ..utils.cosmology import zeldovich_arrays
 from .state import SortContext
 
-MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC, "ewald": _lib.MAC_EWALD}
+MACS = {"ref_x": _lib.MAC_REF_X, "ref_x_bucket": _lib.MAC_REF_X_BUCKET,
+        "periodic": _lib.MAC_PERIODIC, "ewald": _lib.MAC_EWALD}
 EWALD_NT = 64
 
 

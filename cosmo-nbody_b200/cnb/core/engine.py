@@ -10,10 +10,13 @@ kernel is chosen by config.FORCE_MODE:
   "reference"  per-particle stack traversal with the reference's opening
                test (config.PRECISION "f64" = the reference's arithmetic,
                "f32" = float32);
-  "grouped"    warp-per-bucket traversal (config.MAC "ref_x" or "periodic",
-               optional per-bucket theta from `theta_per_group`; "ewald" = the
-               periodic force law, not the reference's minimum image); with
-               config.SUPER_BODIES > 0 and the "ref_x" test, the two-level
+  "grouped"    warp-per-bucket traversal (config.MAC "ref_x": the reference's
+               opening decisions body by body, so every body gets the
+               reference's node set; "ref_x_bucket": the reference's test
+               decided once per bucket, finer node sets; "periodic";
+               "ewald" = the periodic force law, not the reference's minimum
+               image; optional per-bucket theta from `theta_per_group`); with
+               config.SUPER_BODIES > 0 and a reference test, the two-level
                form (super-buckets of that many bodies walk the top of the
                tree once for all their buckets).
 
@@ -29,7 +32,8 @@ from ..utils.cosmology import get_hubble_param
 from .camera import Camera
 from .octree import OctreeManager
 
-MACS = {"ref_x": _lib.MAC_REF_X, "periodic": _lib.MAC_PERIODIC, "ewald": _lib.MAC_EWALD}
+MACS = {"ref_x": _lib.MAC_REF_X, "ref_x_bucket": _lib.MAC_REF_X_BUCKET,
+        "periodic": _lib.MAC_PERIODIC, "ewald": _lib.MAC_EWALD}
 EWALD_NT = 64   # Ewald correction table: 65^3 points on [0, 1/2]^3
 
 
@@ -85,13 +89,14 @@ class SimulationEngine:
 
     def set_super_bodies(self, super_bodies):
         """Two-level walk with super-buckets of at most `super_bodies` bodies
-        (0: single level).  Needs the grouped mode and the "ref_x" test."""
+        (0: single level).  Needs the grouped mode and the reference's test
+        ("ref_x" or "ref_x_bucket")."""
         super_bodies = int(super_bodies)
         if super_bodies == 0:
             self.super_bodies, self.super_ws = 0, None
             return
-        if self.force_mode != "grouped" or self.mac != _lib.MAC_REF_X:
-            raise ValueError("SUPER_BODIES needs FORCE_MODE 'grouped' and MAC 'ref_x'")
+        if self.force_mode != "grouped" or self.mac not in (_lib.MAC_REF_X, _lib.MAC_REF_X_BUCKET):
+            raise ValueError("SUPER_BODIES needs FORCE_MODE 'grouped' and MAC 'ref_x' or 'ref_x_bucket'")
         nbytes = int(_lib.load().cnb_two_level_workspace_bytes(self.state.n, super_bodies))
         if nbytes < 0:
             raise ValueError("SUPER_BODIES must be at least 32")
@@ -130,7 +135,7 @@ class SimulationEngine:
                           tm.node_table.data_ptr(), tm.ranges.data_ptr(), tm.parent.data_ptr(),
                           tm.workspace.data_ptr(), self.super_ws.data_ptr(),
                           self.super_ws.numel() * 4, self.super_bodies, s.force.data_ptr(), s.n,
-                          float(cfg.THETA), self.bodies_per_lane, self.block_warps, float(cfg.G),
+                          float(cfg.THETA), self.mac, self.bodies_per_lane, self.block_warps, float(cfg.G),
                           float(cfg.SOFTENING), float(cfg.BOX_SIZE), self.stats.data_ptr(), status, st)
                 return
             _lib.call("cnb_forces_grouped", px.data_ptr(), py.data_ptr(), pz.data_ptr(),

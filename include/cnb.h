@@ -46,9 +46,14 @@ extern "C" {
 #define CNB_KEY_MORTON63 1 /* full 21-bit interleave, coordinates clamped to [0, 2^21-1] */
 
 /* opening criteria */
-#define CNB_MAC_REF_X 0    /* physics_kernels.py:131-136: x-extent, clamped to box when > box/2 */
+#define CNB_MAC_REF_X 0    /* physics_kernels.py:131-136: x-extent, clamped to box when > box/2,
+                            decided per body (the grouped forms give every body the reference's
+                            own node set) */
 #define CNB_MAC_PERIODIC 1 /* 3-D extent, and open any node whose image is ambiguous for a target */
 #define CNB_MAC_EWALD 2    /* periodic (Ewald) force law, 3-D extent: cnb_forces_grouped_ewald */
+#define CNB_MAC_REF_X_BUCKET 3 /* the reference's test decided once per bucket against the bucket's
+                                  box (a node opens unless every body of the bucket would accept
+                                  it): finer node sets than the reference's, not its forces */
 
 /* arithmetic of the per-particle traversal */
 #define CNB_PREC_F32 0
@@ -259,7 +264,14 @@ int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
  * interaction list, float32 with rsqrt, the minimum image per pair only
  * where a bucket's bodies can see different images.  theta_per_bucket
  * (device float per bucket slot, may be NULL) overrides theta.  mac:
- * CNB_MAC_REF_X or CNB_MAC_PERIODIC.  bodies_per_lane: 1 or 2 (buckets of
+ * CNB_MAC_REF_X (each body gets exactly the nodes the reference's per-body
+ * walk applies: the opening test is decided per body wherever the bucket's
+ * box cannot decide it for all, in float64 where float32 rounding could
+ * change it), CNB_MAC_REF_X_BUCKET or CNB_MAC_PERIODIC; forces are float32
+ * sums.  For CNB_MAC_REF_X the reference's 64-entry stack limit
+ * (physics_kernels.py:143-149, children silently dropped) is not
+ * reproduced: it binds only on trees deeper than about 63 levels.
+ * bodies_per_lane: 1 or 2 (buckets of
  * up to 32 or 64 bodies); block_warps: 2, 4 or 8 warps per block.  slab_mass
  * (CNB_MAC_PERIODIC only): nodes whose image differs between a bucket's
  * bodies are opened unless their mass is at most slab_mass, in which case
@@ -274,7 +286,8 @@ int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                        unsigned long long *stats, int32_t *status, void *stream);
 
 /* Two-level form of cnb_forces_grouped (no reference counterpart; same
- * results as CNB_MAC_REF_X up to float32 summation order).  The tree is cut
+ * results as the one-level walk with the same mac, CNB_MAC_REF_X or
+ * CNB_MAC_REF_X_BUCKET, up to float32 summation order).  The tree is cut
  * into super-buckets (maximal subtrees of at most super_bodies bodies, >= 32);
  * one warp per super-bucket walks the top of the tree once and keeps the
  * nodes every bucket inside it accepts (applied by each bucket from that
@@ -287,7 +300,7 @@ int64_t cnb_two_level_workspace_bytes(int64_t n, int super_bodies);
 int cnb_forces_two_level(const float *px, const float *py, const float *pz,
                          const float *node_table, const int32_t *ranges, const int32_t *parents,
                          int32_t *workspace, void *super_ws, int64_t super_ws_bytes,
-                         int super_bodies, float *force, int64_t n, double theta,
+                         int super_bodies, float *force, int64_t n, double theta, int mac,
                          int bodies_per_lane, int block_warps, double G, double soft, double box,
                          unsigned long long *stats, int32_t *status, void *stream);
 

@@ -270,7 +270,7 @@ static void force_one(const float *px, const float *py, const float *pz, const i
                       const float *n_mass, const float *n_com, const float *n_min,
                       const float *n_max, double theta, double G, double soft, double box,
                       int32_t root, int64_t i, double acc[3], int64_t *overflow,
-                      int64_t *visits) {
+                      int64_t *visits, int64_t *accepted) {
     float x = px[i], y = py[i], z = pz[i];
     double ax = 0.0, ay = 0.0, az = 0.0;
     int32_t stack[64];
@@ -295,6 +295,7 @@ static void force_one(const float *px, const float *py, const float *pz, const i
         double sx = ((double)sxf > box * 0.5) ? box : (double)sxf;
         int mac_pass = (sx * sx) < (theta_sq * d2);
         if (is_leaf || mac_pass) {
+            if (accepted) (*accepted)++;
             if (d2 > 1e-7) {
                 double d_inv = 1.0 / sqrt(d2 + soft * soft);
                 double f = G * (double)nm * (d_inv * d_inv * d_inv);
@@ -318,27 +319,30 @@ static void force_one(const float *px, const float *py, const float *pz, const i
 
 /* compute_forces over targets off .. off+count-1; force is [N,3] float32.
  * Returns the number of stack drops; *visits (optional) receives the total
- * number of popped nodes. */
+ * number of popped nodes, *accepted_out (optional) the number of (body, node)
+ * pairs the opening test accepted (leaves included, before the d2 cut). */
 int64_t orc_compute_forces(const float *px, const float *py, const float *pz,
                            const int32_t *children, const float *n_mass, const float *n_com,
                            const float *n_min, const float *n_max, float *force, double theta,
                            double G, double soft, double box, int32_t root, int64_t off,
-                           int64_t count, int nthreads, int64_t *visits_out) {
-    int64_t overflow = 0, visits = 0;
+                           int64_t count, int nthreads, int64_t *visits_out,
+                           int64_t *accepted_out) {
+    int64_t overflow = 0, visits = 0, accepted = 0;
 #ifdef _OPENMP
     if (nthreads <= 0) nthreads = omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(+ : overflow, visits)
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads) reduction(+ : overflow, visits, accepted)
 #endif
     for (int64_t t = 0; t < count; ++t) {
         double acc[3];
         int64_t i = off + t;
         force_one(px, py, pz, children, n_mass, n_com, n_min, n_max, theta, G, soft, box, root, i,
-                  acc, &overflow, &visits);
+                  acc, &overflow, &visits, &accepted);
         force[3 * i] = (float)acc[0];
         force[3 * i + 1] = (float)acc[1];
         force[3 * i + 2] = (float)acc[2];
     }
     if (visits_out) *visits_out = visits;
+    if (accepted_out) *accepted_out = accepted;
     return overflow;
 }
 
@@ -355,7 +359,7 @@ int64_t orc_forces_targets_f64(const float *px, const float *py, const float *pz
 #endif
     for (int64_t t = 0; t < nt; ++t)
         force_one(px, py, pz, children, n_mass, n_com, n_min, n_max, theta, G, soft, box, root,
-                  targets[t], out + 3 * t, &overflow, NULL);
+                  targets[t], out + 3 * t, &overflow, NULL, NULL);
     return overflow;
 }
 

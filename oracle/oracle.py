@@ -61,7 +61,7 @@ def lib():
     L.orc_compute_forces.restype = C.c_int64
     L.orc_compute_forces.argtypes = [_f32p, _f32p, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p,
                                      _f32p, _d, _d, _d, _d, C.c_int32, _i64, _i64, C.c_int,
-                                     C.POINTER(C.c_int64)]
+                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.orc_forces_targets_f64.restype = C.c_int64
     L.orc_forces_targets_f64.argtypes = [_f32p, _f32p, _f32p, _i32p, _f32p, _f32p, _f32p, _f32p,
                                          _d, _d, _d, _d, C.c_int32, _i64p, _i64, _f64p, C.c_int]
@@ -152,19 +152,23 @@ def build_top_tree_cache(children, root, cache_size=256):
 
 
 def compute_forces(px, py, pz, children, n_mass, n_com, n_min, n_max, theta, G, soft, box,
-                   root, off=0, count=None, nthreads=0):
+                   root, off=0, count=None, nthreads=0, return_accepted=False):
     """physics_kernels.py:14-153 over targets [off, off+count).  Returns
-    (force float32[N,3] with only that range written, stack_drops, visits)."""
+    (force float32[N,3] with only that range written, stack_drops, visits),
+    plus the number of accepted (body, node) pairs when return_accepted."""
     px, py, pz = _f32(px), _f32(py), _f32(pz)
     n = px.size
     if count is None:
         count = n - off
     force = np.zeros((n, 3), np.float32)
     visits = C.c_int64(0)
+    accepted = C.c_int64(0)
     drops = lib().orc_compute_forces(px, py, pz, np.ascontiguousarray(children, np.int32),
                                      _f32(n_mass), _f32(n_com), _f32(n_min), _f32(n_max), force,
                                      theta, G, soft, box, int(root), off, count, nthreads,
-                                     C.byref(visits))
+                                     C.byref(visits), C.byref(accepted))
+    if return_accepted:
+        return force, int(drops), int(visits.value), int(accepted.value)
     return force, int(drops), int(visits.value)
 
 

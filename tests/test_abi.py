@@ -56,7 +56,9 @@ def test_host_only_entry_points():
     assert lib.cnb_two_level_workspace_bytes(1000, 16) == -1
     assert lib.cnb_two_level_workspace_bytes(1 << 21, 1024) > 16 * (1 << 21)
     assert lib.cnb_forces_two_level(None, None, None, None, None, None, None, None, 0, 1024, None,
-                                    5, 0.5, 1, 8, 1.0, 0.01, 1.0, None, None, None) == _lib.CNB_E_INVALID_ARG
+                                    5, 0.5, 0, 1, 8, 1.0, 0.01, 1.0, None, None, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_forces_two_level(None, None, None, None, None, None, None, None, 0, 1024, None,
+                                    5, 0.5, 1, 1, 8, 1.0, 0.01, 1.0, None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_sort_pairs(None, None, None, None, None, 5, 30, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_ctx_take_flags(None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_ctx_set_sort_mode(None, _lib.SORT_ADAPTIVE) == _lib.CNB_E_INVALID_ARG

@@ -1,6 +1,7 @@
 """Two-level grouped traversal (cnb_forces_two_level): super-buckets walk the
 top of the tree once for all their buckets.  It accepts the same nodes as the
-single-level traversal with the reference opening test, so its forces equal
+single-level traversal with the same form of the reference's opening test
+(per body, CNB_MAC_REF_X = 0, or per bucket, CNB_MAC_REF_X_BUCKET = 3), so its forces equal
 cnb_forces_grouped's up to float32 summation order and its interaction count
 is the same; at theta = 0 it is the minimum-image direct sum.  Super-buckets
 whose lists do not fit fall back to the walk from the root."""
@@ -56,7 +57,7 @@ def _bodies(kind, n_grid, seed):
 
 
 class Case:
-    def __init__(self, kind, n_grid, seed=0, bpl=1, soft=None):
+    def __init__(self, kind, n_grid, seed=0, bpl=1, soft=None, mac=0):
         from cnb.core.octree import OctreeManager
         pos, codes = _bodies(kind, n_grid, seed)
         self.pos_h = pos
@@ -68,6 +69,7 @@ class Case:
         self.tm.build(self.P, self.M, torch.from_numpy(codes).cuda())
         self.soft = 0.5 / n_grid if soft is None else soft
         self.st = int(torch.cuda.current_stream().cuda_stream)
+        self.mac = mac
 
     def single(self, theta, warps=4):
         from cnb import _lib
@@ -75,7 +77,7 @@ class Case:
         stats = torch.zeros(4, dtype=torch.int64, device="cuda")
         status = torch.zeros(1, dtype=torch.int32, device="cuda")
         _lib.call("cnb_forces_grouped", *(p.data_ptr() for p in self.P), self.tm.node_table.data_ptr(),
-                  self.tm.workspace.data_ptr(), f.data_ptr(), self.n, theta, None, _lib.MAC_REF_X,
+                  self.tm.workspace.data_ptr(), f.data_ptr(), self.n, theta, None, self.mac,
                   self.bpl, warps, 1.0, self.soft, 1.0, 0.0, stats.data_ptr(), status.data_ptr(), self.st)
         torch.cuda.synchronize()
         assert int(status.item()) == 0
@@ -92,7 +94,7 @@ class Case:
         status = torch.zeros(1, dtype=torch.int32, device="cuda")
         _lib.call("cnb_forces_two_level", *(p.data_ptr() for p in self.P), self.tm.node_table.data_ptr(),
                   self.tm.ranges.data_ptr(), self.tm.parent.data_ptr(), self.tm.workspace.data_ptr(),
-                  ws.data_ptr(), nbytes, super_bodies, f.data_ptr(), self.n, theta, self.bpl, warps,
+                  ws.data_ptr(), nbytes, super_bodies, f.data_ptr(), self.n, theta, self.mac, self.bpl, warps,
                   1.0, self.soft, 1.0, stats.data_ptr(), status.data_ptr(), self.st)
         torch.cuda.synchronize()
         assert int(status.item()) == 0
@@ -107,11 +109,12 @@ def _close(f2, f1, rel=2e-4):
     assert err.max() <= rel * rms, (err.max() / rms)
 
 
+@pytest.mark.parametrize("mac", [0, 3])
 @pytest.mark.parametrize("kind,n_grid,bpl,super_bodies", [
     ("zeldovich", 32, 1, 1024), ("zeldovich", 32, 2, 512), ("clustered", 32, 1, 256),
     ("clustered", 24, 2, 2048), ("zeldovich", 16, 1, 64)])
-def test_same_nodes_as_single_level(kind, n_grid, bpl, super_bodies):
-    c = Case(kind, n_grid, 1, bpl)
+def test_same_nodes_as_single_level(kind, n_grid, bpl, super_bodies, mac):
+    c = Case(kind, n_grid, 1, bpl, mac=mac)
     f1, s1 = c.single(0.5)
     f2, s2, hdr = c.two_level(0.5, super_bodies)
     _close(f2, f1)
@@ -121,9 +124,10 @@ def test_same_nodes_as_single_level(kind, n_grid, bpl, super_bodies):
     assert int(hdr[2]) < int(hdr[0])  # and most of them fit their lists
 
 
+@pytest.mark.parametrize("mac", [0, 3])
 @pytest.mark.parametrize("theta", [0.3, 0.7, 1.0])
-def test_theta_range(theta):
-    c = Case("zeldovich", 24, 2)
+def test_theta_range(theta, mac):
+    c = Case("zeldovich", 24, 2, mac=mac)
     f1, s1 = c.single(theta)
     f2, s2, _ = c.two_level(theta, 1024)
     _close(f2, f1)
@@ -140,14 +144,15 @@ def test_theta_zero_is_direct_sum():
     _close(f2, d, 1e-4)
 
 
+@pytest.mark.parametrize("mac", [0, 3])
 @pytest.mark.parametrize("bpl", [1, 2])
-def test_cut_close_pairs(bpl):
+def test_cut_close_pairs(bpl, mac):
     """The reference's cut (no force from a node at d^2 <= 1e-7): with a small
     softening the planted pairs inside the cut would dominate the force if
     they were applied, and those just outside it must be.  Both traversals at
     theta -> 0 (every entry a leaf) are the direct sum with the cut; at
     theta = 0.5 they accept the same nodes and agree."""
-    c = Case("close_pairs", 16, 2, bpl, soft=1e-4)
+    c = Case("close_pairs", 16, 2, bpl, soft=1e-4, mac=mac)
     m = np.full(c.n, 1.0 / c.n, np.float32)
     d = orc.direct_sum(*c.pos_h, m, np.arange(c.n), 1.0, c.soft)
     f1, _ = c.single(1e-6)
@@ -210,7 +215,8 @@ def test_tiny_systems(n):
         status = torch.zeros(1, dtype=torch.int32, device="cuda")
         _lib.call("cnb_forces_two_level", *(q.data_ptr() for q in P), tm.node_table.data_ptr(),
                   tm.ranges.data_ptr(), tm.parent.data_ptr(), tm.workspace.data_ptr(), ws.data_ptr(),
-                  nbytes, 32, f2.data_ptr(), n, theta, 1, 4, 1.0, 0.01, 1.0, None, status.data_ptr(), st)
+                  nbytes, 32, f2.data_ptr(), n, theta, _lib.MAC_REF_X, 1, 4, 1.0, 0.01, 1.0, None,
+                  status.data_ptr(), st)
         _lib.call("cnb_forces_grouped", *(q.data_ptr() for q in P), tm.node_table.data_ptr(),
                   tm.workspace.data_ptr(), f1.data_ptr(), n, theta, None, _lib.MAC_REF_X, 1, 4, 1.0,
                   0.01, 1.0, 0.0, None, status.data_ptr(), st)
