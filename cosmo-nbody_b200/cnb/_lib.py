@@ -60,6 +60,7 @@ SIGNATURES = {
     "cnb_sort_pairs": (_int, [_p, _p, _p, _p, _p, _i64, _int, _p]),
     "cnb_sort_pairs_noalloc": (_int, [_p, _p, _p, _p, _i64, _int, _p]),
     "cnb_ctx_set_sort_mode": (_int, [_p, _int]),
+    "cnb_ctx_inject_sort_faults": (_int, [_p, _i32, _i64, _i64]),
     "cnb_ctx_sort_stats": (_int, [_p, _p]),
     "cnb_ctx_take_flags": (_int, [_p, _p, _p]),
     "cnb_gather_f32": (_int, [_p, _int, _p, _p, _i64, _p]),

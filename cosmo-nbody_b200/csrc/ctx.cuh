@@ -20,6 +20,10 @@ struct cnb_ctx {
     void *near = nullptr;
     unsigned long long *sort_stats = nullptr;  // [near-sorted path taken, full radix sorts run]
     cudaStream_t side = nullptr;    // captures the full sort into a conditional graph node
+    // cnb_ctx_inject_sort_faults (tests of the failure paths; off by default):
+    int32_t wait_limit = 0;          // look-back polls before a wait gives up (0: 2^22)
+    int64_t withheld_tile = -1;      // one-sweep tile that never publishes its counts
+    int64_t near_dest_bias = 0;      // added to the near-sorted path's R destinations
     // grouped traversal scratch (grown on demand by cnb_forces_grouped)
     void *group_scratch = nullptr;
     size_t group_scratch_bytes = 0;
@@ -45,6 +49,25 @@ constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys per tile
 constexpr int kSweepPasses = 8;                        // 8-bit digits of keys up to 64 bits
 constexpr int64_t kSweepMetaWords = kSweepPasses * 256 + 64;  // counts, tile counters, padding
 // bytes of the one-sweep scratch for up to n_max keys (tiles of 2048 keys)
+// The buffers of one (key, index) sort may be the same array -- keys_in ==
+// keys_out or idx_in == perm_out: the sort then runs at least two passes, so
+// no pass reads what it writes -- but may not overlap in any other way.
+inline bool sort_buffers_ok(const void *keys_in, const void *keys_out, const void *idx_in,
+                            const void *perm_out, int64_t n) {
+    struct R {
+        const char *p;
+        int64_t b;
+    };
+    const R k_in{static_cast<const char *>(keys_in), 8 * n};
+    const R k_out{static_cast<const char *>(keys_out), 8 * n};
+    const R i_in{static_cast<const char *>(idx_in), idx_in ? 4 * n : 0};
+    const R p_out{static_cast<const char *>(perm_out), 4 * n};
+    auto overlap = [](R a, R b) { return a.b > 0 && b.b > 0 && a.p < b.p + b.b && b.p < a.p + a.b; };
+    if (overlap(k_in, k_out) && k_in.p != k_out.p) return false;
+    if (overlap(i_in, p_out) && i_in.p != p_out.p) return false;
+    return !overlap(k_in, i_in) && !overlap(k_in, p_out) && !overlap(k_out, i_in) &&
+           !overlap(k_out, p_out);
+}
 inline int64_t sweep_bytes(int64_t n_max) {
     const int64_t tiles = (n_max + 2047) / 2048;
     return kSweepMetaWords * 4 + (int64_t)kSweepPasses * tiles * 256 * 8;

@@ -306,7 +306,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_onesweep(const uint64_t *__re
                                                            const uint32_t *__restrict__ hist,
                                                            uint64_t *lookback,
                                                            int32_t *tile_counter,
-                                                           int32_t *flags, const int32_t *skip) {
+                                                           int32_t *flags, const int32_t *skip,
+                                                           int wait_limit, int64_t withheld) {
     static_assert(kSweepThreads >= 256, "one thread per digit");
     if (skip && *(volatile const int32_t *)skip) return;
     constexpr int W = kSweepThreads / 32;
@@ -367,10 +368,13 @@ __global__ void __launch_bounds__(kSweepThreads) k_onesweep(const uint64_t *__re
             }
             // publish this tile's count, then add up the earlier tiles' counts
             uint64_t *mine = lookback + tile * 256 + d;
+            // a withheld tile (cnb_ctx_inject_sort_faults) keeps its counts to
+            // itself: the tiles after it wait until their limit
+            const bool publish = tile != withheld;
             if (tile == 0) {
-                lb_store(mine, kLbPrefix | run);
+                if (publish) lb_store(mine, kLbPrefix | run);
             } else {
-                lb_store(mine, kLbCount | run);
+                if (publish) lb_store(mine, kLbCount | run);
                 // kLookbackWindow earlier tiles per round trip, used in order up
                 // to the first one not yet published (tile 0 always ends the walk)
                 int64_t j = tile - 1;
@@ -394,14 +398,14 @@ __global__ void __launch_bounds__(kSweepThreads) k_onesweep(const uint64_t *__re
                     if (done) break;
                     j -= used;
                     if (used == 0) {
-                        if (++spins > kLookbackSpinLimit) {
+                        if (++spins > wait_limit) {
                             set_flag(flags, CNB_FLAG_WAIT_LIMIT);
                             break;
                         }
                         if (spins > 16) __nanosleep(64);
                     }
                 }
-                lb_store(mine, kLbPrefix | (before + run));
+                if (publish) lb_store(mine, kLbPrefix | (before + run));
             }
             gbase[d] = digit_start + before;
         }
@@ -452,7 +456,7 @@ int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_ou
     if (n == 0) return CNB_OK;
     int passes = (key_bits + 7) / 8;
     if (passes < 1) passes = 1;
-    if (passes == 1 && keys_in == keys_out) passes = 2;
+    if (passes == 1 && (keys_in == keys_out || (idx_in && idx_in == perm_out))) passes = 2;
     const int64_t tiles = (n + kSweepTile - 1) / kSweepTile;
     uint32_t *hist = ctx->sweep;
     int32_t *counters = reinterpret_cast<int32_t *>(ctx->sweep + kSweepPasses * 256);
@@ -477,6 +481,7 @@ int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_ou
     CNB_TRY(launch_status());
     const uint64_t *ks = keys_in;
     const uint32_t *vs = idx_in;
+    const int wait_limit = ctx->wait_limit > 0 ? ctx->wait_limit : kLookbackSpinLimit;
     for (int p = 0; p < passes; ++p) {
         const bool last = (p == passes - 1);
         uint64_t *kd = last ? keys_out : ctx->keys_tmp[p & 1];
@@ -484,10 +489,12 @@ int sort_pairs_onesweep(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_ou
         uint64_t *lb = lookback + (int64_t)p * tiles * 256;
         if (vs == nullptr)
             k_onesweep<true><<<(unsigned)tiles, kSweepThreads, kSweepSmem, st>>>(
-                ks, nullptr, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags, skip);
+                ks, nullptr, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags, skip,
+                wait_limit, ctx->withheld_tile);
         else
             k_onesweep<false><<<(unsigned)tiles, kSweepThreads, kSweepSmem, st>>>(
-                ks, vs, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags, skip);
+                ks, vs, kd, vd, n, 8 * p, hist + 256 * p, lb, counters + p, ctx->flags, skip,
+                wait_limit, ctx->withheld_tile);
         CNB_TRY(launch_status());
         ks = kd;
         vs = vd;
@@ -517,7 +524,7 @@ int sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
     if (n == 0) return CNB_OK;
     int passes = (key_bits + 7) / 8;
     if (passes < 1) passes = 1;
-    if (passes == 1 && keys_in == keys_out) passes = 2;
+    if (passes == 1 && (keys_in == keys_out || (idx_in && idx_in == perm_out))) passes = 2;
     const int64_t tiles = (n + kSortTile - 1) / kSortTile;
     // the scatter's staging tile is above the 48 KB default (cheap host call)
     CNB_CUDA(cudaFuncSetAttribute(k_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -623,6 +630,7 @@ extern "C" int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *k
     if (!ctx || n < 0 || key_bits < 1 || key_bits > 64) return CNB_E_INVALID_ARG;
     if (n > ctx->n_max) return CNB_E_TOO_LARGE;
     if (n > 0 && (!keys_in || !keys_out || !perm_out)) return CNB_E_INVALID_ARG;
+    if (!cnb::sort_buffers_ok(keys_in, keys_out, idx_in, perm_out, n)) return CNB_E_INVALID_ARG;
     cudaStream_t st = cnb::as_stream(stream);
     const int32_t *skip = nullptr, *never = nullptr;
     if (!(ctx->sort_mode == CNB_SORT_ADAPTIVE && n > 0 && idx_in == nullptr && keys_in != keys_out))
@@ -673,6 +681,16 @@ extern "C" int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *k
 extern "C" int cnb_ctx_set_sort_mode(cnb_ctx *ctx, int mode) {
     if (!ctx || (mode != CNB_SORT_FULL && mode != CNB_SORT_ADAPTIVE)) return CNB_E_INVALID_ARG;
     ctx->sort_mode = mode;
+    return CNB_OK;
+}
+
+extern "C" int cnb_ctx_inject_sort_faults(cnb_ctx *ctx, int32_t wait_limit,
+                                          int64_t withheld_tile, int64_t near_dest_bias) {
+    if (!ctx || wait_limit < 0 || withheld_tile < -1 || near_dest_bias < 0)
+        return CNB_E_INVALID_ARG;
+    ctx->wait_limit = wait_limit;
+    ctx->withheld_tile = withheld_tile;
+    ctx->near_dest_bias = near_dest_bias;
     return CNB_OK;
 }
 

@@ -559,7 +559,7 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const uint64_t *__r
                                                              int64_t n, NearWs w,
                                                              uint64_t *__restrict__ keys_out,
                                                              uint32_t *__restrict__ perm_out,
-                                                             int32_t *flags) {
+                                                             int32_t *flags, int64_t dest_bias) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t *rk = reinterpret_cast<uint64_t *>(smem);
     uint32_t *rp = reinterpret_cast<uint32_t *>(smem + kNearTile * sizeof(uint64_t));
@@ -571,7 +571,9 @@ __global__ void __launch_bounds__(kNearThreads) k_near_place(const uint64_t *__r
     const int lo = (int)w.tlo[t], hi = (int)w.tlo[t + 1];
     const uint32_t soff = w.soff[t];
     const int s_tile = (int)(w.soff[t + 1] - soff);
-    const int64_t r_before = base - (int64_t)soff;
+    // dest_bias: 0 except under cnb_ctx_inject_sort_faults, which shifts every
+    // destination to exercise the destination checks below
+    const int64_t r_before = base - (int64_t)soff + dest_bias;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     if (s_tile == 0 && lo == hi) {
         // every key of the tile is R and no S key falls among them: a shifted copy
@@ -677,7 +679,8 @@ int sort_pairs_near(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
     k_near_take<<<(unsigned)nt, kNearThreads, 0, st>>>(keys_in, nt, w);
     CNB_TRY(launch_status());
     k_near_place<<<(unsigned)nt, kNearThreads, kNearPlaceSmem, st>>>(keys_in, n, w, keys_out,
-                                                                      perm_out, ctx->flags);
+                                                                      perm_out, ctx->flags,
+                                                                      ctx->near_dest_bias);
     CNB_TRY(launch_status());
     *skip_full = w.ctl + 1;
     *never = w.ctl + 7;  // zeroed with the rest of ctl, never set

@@ -8,14 +8,20 @@
 // below, sized for at most CNB_NOALLOC_MAX_KEYS keys.  Every GPU that loads
 // libcnb.so holds this array (about 24.3 MiB) until the process exits.
 //
+// The sort is the reduce-then-scan form (three launches per 8-bit pass: 24
+// for 63-bit keys, 12 for 30-bit ones), not the one-sweep sort of
+// cnb_sort_pairs; both are stable, so the output is identical.
+//
 // The array's host-side name is only a stand-in for the device symbol: host
 // code must not pass it to a kernel.  The first call on each device looks up
 // the device address with cudaGetSymbolAddress (with that device current)
-// and caches it; that first call should therefore come before any stream
-// capture.  All calls share the one array and it keeps the last call's
-// contents: nothing in it has to start at zero (each pass writes every count
-// it reads), and calls whose work overlaps on the GPU -- on different
-// streams, or from different host threads -- race on it.
+// and caches it for the life of the process; that first call should
+// therefore come before any stream capture, and a device reset
+// (cudaDeviceReset) after it is not supported: the cached address would
+// outlive the module it points into.  All calls share the one array and it
+// keeps the last call's contents: nothing in it has to start at zero (each
+// pass writes every count it reads), and calls whose work overlaps on the
+// GPU -- on different streams, or from different host threads -- race on it.
 #include <mutex>
 
 #include "ctx.cuh"
@@ -66,6 +72,7 @@ extern "C" int cnb_sort_pairs_noalloc(const uint64_t *keys_in, uint64_t *keys_ou
     if (n > cnb::kMaxKeys) return CNB_E_TOO_LARGE;
     if (n == 0) return CNB_OK;
     if (!keys_in || !keys_out || !perm_out) return CNB_E_INVALID_ARG;
+    if (!cnb::sort_buffers_ok(keys_in, keys_out, idx_in, perm_out, n)) return CNB_E_INVALID_ARG;
     unsigned char *base = nullptr;
     CNB_TRY(cnb::scratch_address(&base));
     // a view of the fixed array shaped like a context: nothing is allocated

@@ -84,6 +84,9 @@ int cnb_ctx_destroy(cnb_ctx *ctx);
  * sort of (key, index) pairs.  keys_out receives the sorted keys, perm_out
  * the original index of each sorted key.  idx_in may be NULL (identity).
  * key_bits = number of low key bits that may be non-zero (30 or 63).
+ * keys_out may be keys_in and perm_out may be idx_in (at least two passes
+ * then run); any other overlap between the four arrays is rejected
+ * (CNB_E_INVALID_ARG).
  * One kernel per 8-bit digit: each 4096-key tile finds where its keys go by
  * looking back at the counts earlier tiles publish; the waits are bounded,
  * and a wait that gives up raises CNB_FLAG_WAIT_LIMIT in the context
@@ -91,6 +94,19 @@ int cnb_ctx_destroy(cnb_ctx *ctx);
 int cnb_sort_pairs(cnb_ctx *ctx, const uint64_t *keys_in, uint64_t *keys_out,
                    const uint32_t *idx_in, uint32_t *perm_out, int64_t n, int key_bits,
                    void *stream);
+
+/* No counterpart in the reference.  Test hook for the sort's failure paths
+ * (all off by default): wait_limit > 0 bounds every look-back wait of the
+ * one-sweep sort at that many polls (0: the default 2^22); withheld_tile >= 0
+ * makes that 4096-key tile of every pass keep its digit counts to itself, so
+ * the tiles after it wait until their limit, give up and raise
+ * CNB_FLAG_WAIT_LIMIT (-1: off); near_dest_bias > 0 shifts every destination
+ * of the near-sorted path's placement by that many keys, so its destination
+ * check skips the writes that leave the array and raises
+ * CNB_FLAG_SORT_CHECK.  Results are invalid while a fault is injected; the
+ * context stays usable once the hook is reset with (0, -1, 0). */
+int cnb_ctx_inject_sort_faults(cnb_ctx *ctx, int32_t wait_limit, int64_t withheld_tile,
+                               int64_t near_dest_bias);
 
 /* No counterpart in the reference.  Sort mode of a context (default
  * CNB_SORT_FULL).  CNB_SORT_ADAPTIVE: cnb_sort_pairs with idx_in == NULL and
@@ -120,17 +136,20 @@ int cnb_ctx_sort_stats(cnb_ctx *ctx, int64_t *out);
  * ordered, no synchronisation). */
 int cnb_ctx_take_flags(cnb_ctx *ctx, int32_t *status, void *stream);
 
-/* No counterpart in the reference.  The same stable (key, index) sort as
- * cnb_sort_pairs for callers that cannot allocate device memory (a plugin
+/* No counterpart in the reference.  A stable (key, index) sort with output
+ * identical to cnb_sort_pairs', for callers that cannot allocate device memory (a plugin
  * whose host application owns all device memory through its own pool, or
  * code running where a cudaMalloc and the synchronisation it may bring are
  * not allowed).  It takes no context and allocates nothing: its scratch is a
  * fixed device array inside libcnb.so, sized for at most
  * CNB_NOALLOC_MAX_KEYS keys (about 24.3 MiB, held on every GPU that loads the
- * library until the process exits).  Larger n returns CNB_E_TOO_LARGE.  The
- * first call on a device looks up the array's device address (so make it
- * before any stream capture).  All calls share the array: calls that overlap
- * on the GPU race. */
+ * library until the process exits).  Larger n returns CNB_E_TOO_LARGE.  It
+ * runs the reduce-then-scan radix sort: three launches per 8-bit digit (24
+ * for 63-bit keys, 12 for 30-bit keys) where cnb_sort_pairs runs one.  The
+ * first call on a device looks up the array's device address and keeps it
+ * for the life of the process (so make that call before any stream capture;
+ * a cudaDeviceReset after it is not supported).  All calls share the array:
+ * calls that overlap on the GPU race.  Buffer rules as for cnb_sort_pairs. */
 #define CNB_NOALLOC_MAX_KEYS (1 << 20)
 int cnb_sort_pairs_noalloc(const uint64_t *keys_in, uint64_t *keys_out, const uint32_t *idx_in,
                            uint32_t *perm_out, int64_t n, int key_bits, void *stream);

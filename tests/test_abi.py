@@ -62,6 +62,13 @@ def test_host_only_entry_points():
     assert lib.cnb_sort_pairs(None, None, None, None, None, 5, 30, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_ctx_take_flags(None, None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_ctx_set_sort_mode(None, _lib.SORT_ADAPTIVE) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_ctx_inject_sort_faults(None, 10, 3, 0) == _lib.CNB_E_INVALID_ARG
+    # sort buffers: the same array in and out is allowed, any other overlap is
+    # rejected before the device is touched (these addresses are never read)
+    a = 1 << 20
+    assert lib.cnb_sort_pairs_noalloc(a, a + 8, None, a + 4096, 10, 63, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_sort_pairs_noalloc(a, a + 4096, a + 8192, a + 8196, 10, 63, None) == _lib.CNB_E_INVALID_ARG
+    assert lib.cnb_sort_pairs_noalloc(a, a + 4096, None, a + 40, 10, 63, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_ctx_sort_stats(None, None) == _lib.CNB_E_INVALID_ARG
     assert lib.cnb_render_density(None, None, None, None, None, 4, 0, 4, None) == _lib.CNB_E_INVALID_ARG
 

@@ -63,6 +63,46 @@ def test_noalloc_sort_matches_context_sort_twice():
     assert np.all(np.diff(b[0].astype(np.int64)) >= 0)
 
 
+def _noalloc(K, ko, V, po, n, bits):
+    from cnb import _lib
+    st = int(torch.cuda.current_stream().cuda_stream)
+    _lib.call("cnb_sort_pairs_noalloc", K.data_ptr(), ko.data_ptr(), V.data_ptr() if V is not None else None,
+              po.data_ptr(), n, bits, st)
+    torch.cuda.synchronize()
+
+
+def test_noalloc_sort_edge_shapes():
+    """The largest size (the last tile fills the scratch), one 8-bit pass with
+    distinct buffers, one pass in place (keys_out == keys_in, then two passes
+    run), and perm_out == idx_in: every result equals numpy's stable argsort."""
+    rng = np.random.default_rng(77)
+    n = 1 << 20
+    keys = rng.integers(0, 1 << 63, n, dtype=np.uint64)
+    a, b = _sort_both(keys, 63)
+    np.testing.assert_array_equal(b[1].astype(np.int64), np.argsort(keys, kind="stable"))
+    np.testing.assert_array_equal(b[0], a[0])
+    for n, in_place in ((100_003, False), (4096 * 3 + 17, True)):
+        k = rng.integers(0, 256, n, dtype=np.uint64)
+        want = np.argsort(k, kind="stable")
+        K = torch.from_numpy(k).cuda()
+        ko = K if in_place else torch.empty_like(K)
+        po = torch.empty(n, dtype=torch.uint32, device="cuda")
+        _noalloc(K, ko, None, po, n, 8)
+        np.testing.assert_array_equal(po.cpu().numpy().astype(np.int64), want)
+        np.testing.assert_array_equal(ko.cpu().numpy(), k[want])
+    # carried indices sorted in place of themselves
+    n = 50_001
+    k = rng.integers(0, 256, n, dtype=np.uint64)
+    v = rng.permutation(n).astype(np.uint32)
+    K = torch.from_numpy(k).cuda()
+    V = torch.from_numpy(v).cuda()
+    ko = torch.empty_like(K)
+    _noalloc(K, ko, V, V, n, 8)
+    want = np.argsort(k, kind="stable")
+    np.testing.assert_array_equal(V.cpu().numpy(), v[want])
+    np.testing.assert_array_equal(ko.cpu().numpy(), k[want])
+
+
 def test_noalloc_sort_rejects_oversize():
     from cnb import _lib
     lib = _lib.load()
