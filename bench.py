@@ -63,7 +63,7 @@ def parse():
     ap.add_argument("--n-grid", type=int, default=N_GRID)
     ap.add_argument("--theta", type=float, default=0.5)
     ap.add_argument("--force-mode", default="grouped", choices=["grouped", "reference"])
-    ap.add_argument("--mac", default="ref_x", choices=["ref_x", "periodic", "ewald"],
+    ap.add_argument("--mac", default="ref_x", choices=["ref_x", "ref_x_bucket", "periodic", "ewald"],
                     help="opening test; 'ewald' also switches to the periodic force law")
     ap.add_argument("--precision", default="f32", choices=["f32", "f64"],
                     help="arithmetic of the reference force mode (f64 = the reference's)")

@@ -45,7 +45,7 @@ def tune(engine, shapes=SHAPES, supers=SUPERS, reps=3, use_cache=True, save=True
     `engine` (grouped mode, tree already built by forces_only/step).  Returns
     a report dict."""
     key = _key(engine)
-    if engine.mac != 0:          # the two-level walk exists for the reference test only
+    if engine.mac not in (0, 3):   # the two-level walk exists for the reference test only
         supers = (0,)
     cache = _load() if use_cache else {}
     if key in cache and len(cache[key].get("shape", [])) == 3:

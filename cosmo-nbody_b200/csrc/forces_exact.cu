@@ -29,11 +29,15 @@
 // reference.  The forces differ from the reference's only by float32 against
 // float64 arithmetic and summation order.
 //
-// Lists: entries accepted by the whole bucket with one image for all of its
-// bodies and out of the cut's reach (the bulk) are applied as in
-// forces_grouped.cu (packed float2 for two bodies per lane, no image, no
-// cut); every other accepted entry keeps the node's raw CoM and is applied
-// with the per-pair minimum image, the cut and the entry's body mask.
+// Lists: entries with one image for every body of the bucket and out of the
+// cut's reach go to the whole-bucket list (applied as in forces_grouped.cu:
+// packed float2 for two bodies per lane, no image, no cut) or, reached by part
+// of the bucket, to the masked list (the same, the mass selected per body by
+// the entry's mask); every other accepted entry keeps the node's raw CoM and
+// is applied with the per-pair minimum image, the cut and its mask.
+// Per-body items carry the band [lo, hi] around s^2 / theta^2 inside which
+// the float32 d^2 cannot decide, and flags for the per-pair image and the
+// cut, so the common item is a handful of packed operations per body pair.
 //
 // Limit: the reference's 64-entry stack drops children when full
 // (physics_kernels.py:143-149).  That happens only for trees deeper than
@@ -45,12 +49,13 @@ namespace cnb {
 constexpr int kXPStack = 256;           // (node, mask) entries per warp for part of a bucket
 constexpr float kCutLo = 0.99999e-7f, kCutHi = 1.00001e-7f;  // float64 band around the cut
 
+// per-warp shared memory: three lists of kGList entries (whole bucket, masked
+// with one image, anything else) and the per-body items of one round
 template <int BPL> __host__ __device__ constexpr int exact_f4_per_warp() {
-    // full-bucket list, masked list (kGList entries each), per-body items (32 x 2)
-    return 2 * kGList * entry_width<BPL>() + 64;
+    return 3 * kGList * entry_width<BPL>() + 3 * 32;
 }
-constexpr int kExactMasksPerWarp = kGList + 32 + kXPStack;  // uint2
-constexpr int kExactIntsPerWarp = kGStack + kXPStack;         // int32
+constexpr int kExactMasksPerWarp = 2 * kGList + kXPStack;  // uint2
+constexpr int kExactIntsPerWarp = kGStack + kXPStack;       // int32
 
 template <int BPL>
 constexpr size_t exact_smem(int warps) {
@@ -58,17 +63,25 @@ constexpr size_t exact_smem(int warps) {
                             kExactMasksPerWarp * sizeof(uint2) + kExactIntsPerWarp * sizeof(int32_t));
 }
 
-__device__ __forceinline__ float nearest_image(float d) {
-    // rint(d) through the 1.5 * 2^23 rounding constant (|d| < 2^22)
-    return __fsub_rn(__fadd_rn(d, 12582912.f), 12582912.f);
+// per-body item flags
+constexpr int kItemWrap = 1;  // the CoM's minimum image can differ between the bucket's bodies
+constexpr int kItemNear = 2;  // the item is close enough to the bucket for the cut to apply
+
+__device__ __forceinline__ float2 dup2(float a) { return make_float2(a, a); }
+
+// d - rint(d) through the 1.5 * 2^23 rounding constant (|d| < 2^22): the
+// reference's d - round(d), exact in float32 for |d| < 1
+__device__ __forceinline__ float minus_image(float d) {
+    return d - __fsub_rn(__fadd_rn(d, 12582912.f), 12582912.f);
+}
+__device__ __forceinline__ float2 minus_image2(float2 d) {
+    const float2 rc = dup2(12582912.f), nrc = dup2(-12582912.f);
+    return __ffma2_rn(__fadd2_rn(__fadd2_rn(d, rc), nrc), dup2(-1.f), d);
 }
 
-// The reference's test for one body: sx^2 < theta^2 d^2 on float64 values.
-// The float32 form decides unless the two sides are within kRelMargin.
-__device__ __forceinline__ bool ref_accepts(float s, float th2, double th2d, float dx, float dy,
-                                            float dz, float d2) {
-    const float s2 = s * s, t = th2 * d2;
-    if (fabsf(s2 - t) > kRelMargin * t) return s2 < t;
+// The reference's test for one body, sx^2 < theta^2 d^2, in float64: called
+// only when the float32 d^2 lies within the margin band of s^2 / theta^2.
+__device__ __noinline__ bool ref_accepts_f64(float s, double th2d, float dx, float dy, float dz) {
     const double d2d = (double)dx * dx + (double)dy * dy + (double)dz * dz;
     return (double)s * (double)s < th2d * d2d;
 }
@@ -81,10 +94,12 @@ __device__ __forceinline__ bool ref_outside_cut(float dx, float dy, float dz, fl
     return d2d > 1e-7;
 }
 
-// Masked list: cnt entries of raw CoM and mass (two float4 per entry for two
-// bodies per lane, as put_entry writes them) applied to the lane's bodies in
-// the entry's mask, with the per-pair minimum image and the cut.
-template <int BPL>
+// Masked list: cnt entries (two float4 per entry for two bodies per lane, as
+// put_entry writes them) applied to the lane's bodies in the entry's mask.
+// WRAP_CUT: raw CoM with the per-pair minimum image and the cut; otherwise
+// the CoM at the one image every body of the bucket sees, out of the cut's
+// reach.
+template <int BPL, bool WRAP_CUT>
 __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *masks, int cnt,
                                              int lane, const float (&x)[BPL], const float (&y)[BPL],
                                              const float (&z)[BPL], float soft2, float (&ax)[BPL],
@@ -93,9 +108,7 @@ __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *ma
     if constexpr (BPL == 2) {
         const float2 nx = make_float2(-x[0], -x[1]), ny = make_float2(-y[0], -y[1]),
                      nz = make_float2(-z[0], -z[1]);
-        const float2 s2 = make_float2(soft2, soft2);
-        const float2 rc = make_float2(12582912.f, 12582912.f), nrc = make_float2(-12582912.f, -12582912.f);
-        const float2 m1 = make_float2(-1.f, -1.f);
+        const float2 s2 = dup2(soft2);
         float2 fx = make_float2(ax[0], ax[1]), fy = make_float2(ay[0], ay[1]),
                fz = make_float2(az[0], az[1]);
 #pragma unroll 4
@@ -105,15 +118,17 @@ __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *ma
             float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx);
             float2 dy = __fadd2_rn(make_float2(a.z, a.w), ny);
             float2 dz = __fadd2_rn(make_float2(b.x, b.y), nz);
-            dx = __ffma2_rn(__fadd2_rn(__fadd2_rn(dx, rc), nrc), m1, dx);
-            dy = __ffma2_rn(__fadd2_rn(__fadd2_rn(dy, rc), nrc), m1, dy);
-            dz = __ffma2_rn(__fadd2_rn(__fadd2_rn(dz, rc), nrc), m1, dz);
+            if (WRAP_CUT) {
+                dx = minus_image2(dx);
+                dy = minus_image2(dy);
+                dz = minus_image2(dz);
+            }
             const float2 q = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __ffma2_rn(dz, dz, s2)));
-            float r0 = rsqrtf(q.x), r1 = rsqrtf(q.y);
-            r0 = (q.x > cut && ((mk.x >> lane) & 1u)) ? r0 : 0.f;
-            r1 = (q.y > cut && ((mk.y >> lane) & 1u)) ? r1 : 0.f;
-            const float2 r = make_float2(r0, r1);
-            const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(make_float2(b.z, b.w), r), r), r);
+            const bool u0 = (mk.x >> lane) & 1u, u1 = (mk.y >> lane) & 1u;
+            const float2 w = make_float2(u0 && (!WRAP_CUT || q.x > cut) ? b.z : 0.f,
+                                         u1 && (!WRAP_CUT || q.y > cut) ? b.w : 0.f);
+            const float2 r = make_float2(rsqrtf(q.x), rsqrtf(q.y));
+            const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(w, r), r), r);
             fx = __ffma2_rn(f, dx, fx);
             fy = __ffma2_rn(f, dy, fy);
             fz = __ffma2_rn(f, dz, fz);
@@ -125,22 +140,113 @@ __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *ma
 #pragma unroll 4
         for (int j = 0; j < cnt; ++j) {
             const float4 e = list[j];
-            const uint32_t mw = masks[j].x;
+            const bool u = (masks[j].x >> lane) & 1u;
 #pragma unroll
             for (int b = 0; b < BPL; ++b) {
                 float dx = e.x - x[b], dy = e.y - y[b], dz = e.z - z[b];
-                dx -= pair_image(dx);
-                dy -= pair_image(dy);
-                dz -= pair_image(dz);
+                if (WRAP_CUT) {
+                    dx = minus_image(dx);
+                    dy = minus_image(dy);
+                    dz = minus_image(dz);
+                }
                 const float q = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, soft2)));
                 const float r = rsqrtf(q);
-                const float f = (q > cut && ((mw >> lane) & 1u)) ? e.w * r * r * r : 0.f;
+                const float f = (u && (!WRAP_CUT || q > cut)) ? e.w * r * r * r : 0.f;
                 ax[b] = fmaf(f, dx, ax[b]);
                 ay[b] = fmaf(f, dy, ay[b]);
                 az[b] = fmaf(f, dz, az[b]);
             }
         }
     }
+}
+
+// One per-body item for the lane's bodies: I = raw CoM and mass, J = (s,
+// lo, hi, flags) with [lo, hi] the float32 band around s^2 / theta^2 where
+// float64 decides, bodies in (m0, m1).  Adds the force of the bodies that
+// accept; returns which of them open the node.
+template <int BPL>
+__device__ __forceinline__ void per_body_item(float4 I, float4 J, uint32_t m0, uint32_t m1, int lane,
+                                              double th2d, float soft2, const float (&x)[BPL],
+                                              const float (&y)[BPL], const float (&z)[BPL],
+                                              float (&ax)[BPL], float (&ay)[BPL], float (&az)[BPL],
+                                              bool (&opn)[BPL], int &n_acc) {
+    const int flags = __float_as_int(J.w);
+    if constexpr (BPL == 2) {
+        float2 dx = __fadd2_rn(dup2(I.x), make_float2(-x[0], -x[1]));
+        float2 dy = __fadd2_rn(dup2(I.y), make_float2(-y[0], -y[1]));
+        float2 dz = __fadd2_rn(dup2(I.z), make_float2(-z[0], -z[1]));
+        if (flags & kItemWrap) {
+            dx = minus_image2(dx);
+            dy = minus_image2(dy);
+            dz = minus_image2(dz);
+        }
+        const float2 d2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+        bool a0 = d2.x > J.z, a1 = d2.y > J.z;
+        const bool in0 = (m0 >> lane) & 1u, in1 = (m1 >> lane) & 1u;
+        if (in0 && !a0 && !(d2.x < J.y)) a0 = ref_accepts_f64(J.x, th2d, dx.x, dy.x, dz.x);
+        if (in1 && !a1 && !(d2.y < J.y)) a1 = ref_accepts_f64(J.x, th2d, dx.y, dy.y, dz.y);
+        const bool u0 = in0 && a0, u1 = in1 && a1;
+        opn[0] = in0 && !a0;
+        opn[BPL - 1] = in1 && !a1;
+        n_acc += (int)u0 + (int)u1;
+        bool f0 = u0, f1 = u1;
+        if (flags & kItemNear) {
+            f0 = f0 && ref_outside_cut(dx.x, dy.x, dz.x, d2.x);
+            f1 = f1 && ref_outside_cut(dx.y, dy.y, dz.y, d2.y);
+        }
+        const float2 q = __fadd2_rn(d2, dup2(soft2));
+        const float2 r = make_float2(rsqrtf(q.x), rsqrtf(q.y));
+        const float2 w = make_float2(f0 ? I.w : 0.f, f1 ? I.w : 0.f);
+        const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(w, r), r), r);
+        const float2 fx = __ffma2_rn(f, dx, make_float2(ax[0], ax[1]));
+        const float2 fy = __ffma2_rn(f, dy, make_float2(ay[0], ay[1]));
+        const float2 fz = __ffma2_rn(f, dz, make_float2(az[0], az[1]));
+        ax[0] = fx.x; ax[1] = fx.y;
+        ay[0] = fy.x; ay[1] = fy.y;
+        az[0] = fz.x; az[1] = fz.y;
+    } else {
+#pragma unroll
+        for (int b = 0; b < BPL; ++b) {
+            float dx = I.x - x[b], dy = I.y - y[b], dz = I.z - z[b];
+            if (flags & kItemWrap) {
+                dx = minus_image(dx);
+                dy = minus_image(dy);
+                dz = minus_image(dz);
+            }
+            const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            const bool in = ((b == 0 ? m0 : m1) >> lane) & 1u;
+            bool a = d2 > J.z;
+            if (in && !a && !(d2 < J.y)) a = ref_accepts_f64(J.x, th2d, dx, dy, dz);
+            const bool u = in && a;
+            opn[b] = in && !a;
+            n_acc += (int)u;
+            const bool fu = u && (!(flags & kItemNear) || ref_outside_cut(dx, dy, dz, d2));
+            const float r = rsqrtf(d2 + soft2);
+            const float f = fu ? I.w * r * r * r : 0.f;
+            ax[b] = fmaf(f, dx, ax[b]);
+            ay[b] = fmaf(f, dy, ay[b]);
+            az[b] = fmaf(f, dz, az[b]);
+        }
+    }
+}
+
+// Applies the first 32 entries of a list and moves the rest to the front.
+template <int BPL, int KIND>
+__device__ __forceinline__ void flush32(float4 *lst, uint2 *msk, int &cnt, int lane,
+                                        const float (&x)[BPL], const float (&y)[BPL],
+                                        const float (&z)[BPL], float soft2, float (&ax)[BPL],
+                                        float (&ay)[BPL], float (&az)[BPL]) {
+    constexpr int EW = entry_width<BPL>();
+    if (KIND == 0) apply_entries<BPL, false, false>(lst, 32, x, y, z, soft2, ax, ay, az);
+    else if (KIND == 1) apply_masked<BPL, false>(lst, msk, 32, lane, x, y, z, soft2, ax, ay, az);
+    else apply_masked<BPL, true>(lst, msk, 32, lane, x, y, z, soft2, ax, ay, az);
+    __syncwarp();
+#pragma unroll
+    for (int w = 0; w < EW; ++w)
+        if (lane < cnt - 32) lst[EW * lane + w] = lst[EW * (32 + lane) + w];
+    if (KIND != 0 && lane < cnt - 32) msk[lane] = msk[32 + lane];
+    cnt -= 32;
+    __syncwarp();
 }
 
 template <int BPL, int WARPS>
@@ -151,13 +257,14 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
     float4 *f4 = reinterpret_cast<float4 *>(x_smem);
-    float4 *list = f4 + wib * exact_f4_per_warp<BPL>();
-    float4 *mlist = list + kGList * EW;
-    float4 *plist = mlist + kGList * EW;
+    float4 *list = f4 + wib * exact_f4_per_warp<BPL>();  // whole bucket, one image, no cut
+    float4 *mlist = list + kGList * EW;                   // masked, one image, no cut
+    float4 *xlist = mlist + kGList * EW;                  // per-pair image and cut, any mask
+    float4 *plist = xlist + kGList * EW;                  // per-body items (3 float4 each)
     uint2 *mbase = reinterpret_cast<uint2 *>(f4 + WARPS * exact_f4_per_warp<BPL>());
     uint2 *mmask = mbase + wib * kExactMasksPerWarp;
-    uint2 *pmask = mmask + kGList;
-    uint2 *psmask = pmask + 32;
+    uint2 *xmask = mmask + kGList;
+    uint2 *psmask = xmask + kGList;
     int32_t *stack = reinterpret_cast<int32_t *>(mbase + WARPS * kExactMasksPerWarp) +
                      wib * kExactIntsPerWarp;
     int32_t *pstack = stack + kGStack;
@@ -229,11 +336,12 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             th2d = (double)th * (double)th;
         }
         const float th2 = (float)th2d;
+        const float inv_th2 = 1.f / th2;
 
         float ax[BPL], ay[BPL], az[BPL];
 #pragma unroll
         for (int b = 0; b < BPL; ++b) ax[b] = ay[b] = az[b] = 0.f;
-        int top = 1, ptop = 0, cnt = 0, mcnt = 0;
+        int top = 1, ptop = 0, cnt = 0, mcnt = 0, xcnt = 0, n_acc = 0;
         bool seeded = false;
         if (P.super_of_body) {
             const int sup = P.super_of_body[bk.x];
@@ -295,7 +403,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             const bool whole = mk.x == fm.x && mk.y == fm.y;
             // 1: accepted by every body of the mask, 2: opened by every one, 3: per body
             int cls = 0;
-            bool one_image = false;
+            bool one_image = false, zero_image = false, near_box = false;
             float4 A = make_float4(0.f, 0.f, 0.f, 0.f), E = A;
             float s = 0.f;
             int32_t c0 = -1, c1 = -1;
@@ -323,30 +431,41 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                         else if (s2 > th2 * d2max * (1.f + kRelMargin)) cls = 2;
                         else cls = 3;
                     }
-                    one_image = whole && d2min > kCutGuard && adx < wlx && ady < wly && adz < wlz;
+                    near_box = d2min <= kCutGuard;
+                    one_image = adx < wlx && ady < wly && adz < wlz;
+                    zero_image = one_image && sx_ == 0.f && sy_ == 0.f && sz_ == 0.f;
                     E = make_float4(A.x - sx_, A.y - sy_, A.z - sz_, A.w);
                 }
             }
             n_tests += (node >= 0);
-            const uint32_t m_one = __ballot_sync(0xffffffffu, cls == 1 && one_image);
-            const uint32_t m_msk = __ballot_sync(0xffffffffu, cls == 1 && !one_image);
+            const bool to_list = cls == 1 && whole && one_image && !near_box;
+            const bool to_m = cls == 1 && !whole && one_image && !near_box;
+            const bool to_x = cls == 1 && !(one_image && !near_box);
+            const uint32_t m_one = __ballot_sync(0xffffffffu, to_list);
+            const uint32_t m_msk = __ballot_sync(0xffffffffu, to_m);
+            const uint32_t m_x = __ballot_sync(0xffffffffu, to_x);
             const uint32_t m_ow = __ballot_sync(0xffffffffu, cls == 2 && whole);
             const uint32_t m_op = __ballot_sync(0xffffffffu, cls == 2 && !whole);
             const uint32_t m_pb = __ballot_sync(0xffffffffu, cls == 3);
             if (cls == 1) {
                 const int nb = __popc(mk.x) + __popc(mk.y);
                 n_inter += nb;
-                if (one_image) {
+                if (to_list) {
                     put_entry<BPL>(list, cnt + __popc(m_one & lt), E);
-                } else {
+                } else if (to_m) {
                     const int w = mcnt + __popc(m_msk & lt);
-                    put_entry<BPL>(mlist, w, A);
+                    put_entry<BPL>(mlist, w, E);
                     mmask[w] = mk;
+                } else {
+                    const int w = xcnt + __popc(m_x & lt);
+                    put_entry<BPL>(xlist, w, A);
+                    xmask[w] = mk;
                     n_wrap += nb;
                 }
             }
             cnt += __popc(m_one);
             mcnt += __popc(m_msk);
+            xcnt += __popc(m_x);
             const int n_ow = __popc(m_ow), n_op = __popc(m_op);
             if (top + 2 * n_ow > kGStack || ptop + 2 * n_op > kXPStack) {
                 overflow = true;  // children dropped (flagged)
@@ -368,40 +487,27 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             }
             const int pcnt = __popc(m_pb);
             if (cls == 3) {
+                // the band [lo, hi] around s^2 / theta^2 inside which float64 decides
+                const float R = s * s * inv_th2;
+                const int fl = (zero_image ? 0 : kItemWrap) | (near_box ? kItemNear : 0);
                 const int w = __popc(m_pb & lt);
-                plist[2 * w] = A;
-                plist[2 * w + 1] = make_float4(s, __int_as_float(c0), __int_as_float(c1), 0.f);
-                pmask[w] = mk;
+                plist[3 * w] = A;
+                plist[3 * w + 1] = make_float4(s, R * (1.f - kRelMargin), R * (1.f + kRelMargin),
+                                               __int_as_float(fl));
+                plist[3 * w + 2] = make_float4(__int_as_float(c0), __int_as_float(c1),
+                                               __uint_as_float(mk.x), __uint_as_float(mk.y));
             }
             __syncwarp();
             // per-body items: every body of the mask decides for itself
             for (int j = 0; j < pcnt; ++j) {
-                const float4 I = plist[2 * j], J = plist[2 * j + 1];
-                const uint2 pm = pmask[j];
+                const float4 I = plist[3 * j], J = plist[3 * j + 1], K = plist[3 * j + 2];
                 bool opn[BPL];
-#pragma unroll
-                for (int b = 0; b < BPL; ++b) {
-                    const bool inm = (((b == 0 ? pm.x : pm.y) >> lane) & 1u) != 0u;
-                    float dx = I.x - x[b], dy = I.y - y[b], dz = I.z - z[b];
-                    dx -= nearest_image(dx);
-                    dy -= nearest_image(dy);
-                    dz -= nearest_image(dz);
-                    const float d2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    const bool pass = ref_accepts(J.x, th2, th2d, dx, dy, dz, d2);
-                    const bool use = inm && pass;
-                    opn[b] = inm && !pass;
-                    n_inter += use;
-                    n_wrap += use;
-                    const float r = rsqrtf(d2 + soft2);
-                    const float f = (use && ref_outside_cut(dx, dy, dz, d2)) ? I.w * r * r * r : 0.f;
-                    ax[b] = fmaf(f, dx, ax[b]);
-                    ay[b] = fmaf(f, dy, ay[b]);
-                    az[b] = fmaf(f, dz, az[b]);
-                }
+                per_body_item<BPL>(I, J, __float_as_uint(K.z), __float_as_uint(K.w), lane, th2d, soft2,
+                                   x, y, z, ax, ay, az, opn, n_acc);
                 const uint2 om = make_uint2(__ballot_sync(0xffffffffu, opn[0]),
                                             BPL == 2 ? __ballot_sync(0xffffffffu, opn[BPL - 1]) : 0u);
                 if (om.x | om.y) {
-                    const int32_t k0 = __float_as_int(J.y), k1c = __float_as_int(J.z);
+                    const int32_t k0 = __float_as_int(K.x), k1c = __float_as_int(K.y);
                     if (om.x == fm.x && om.y == fm.y) {
                         if (top + 2 > kGStack) {
                             overflow = true;
@@ -427,29 +533,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             }
             max_top = max(max_top, top + ptop);
             __syncwarp();
-            if (cnt >= 32) {
-                apply_entries<BPL, false, false>(list, 32, x, y, z, soft2, ax, ay, az);
-                __syncwarp();
-#pragma unroll
-                for (int w = 0; w < EW; ++w)
-                    if (lane < cnt - 32) list[EW * lane + w] = list[EW * (32 + lane) + w];
-                cnt -= 32;
-                __syncwarp();
-            }
-            if (mcnt >= 32) {
-                apply_masked<BPL>(mlist, mmask, 32, lane, x, y, z, soft2, ax, ay, az);
-                __syncwarp();
-#pragma unroll
-                for (int w = 0; w < EW; ++w)
-                    if (lane < mcnt - 32) mlist[EW * lane + w] = mlist[EW * (32 + lane) + w];
-                if (lane < mcnt - 32) mmask[lane] = mmask[32 + lane];
-                mcnt -= 32;
-                __syncwarp();
-            }
+            if (cnt >= 32) flush32<BPL, 0>(list, nullptr, cnt, lane, x, y, z, soft2, ax, ay, az);
+            if (mcnt >= 32) flush32<BPL, 1>(mlist, mmask, mcnt, lane, x, y, z, soft2, ax, ay, az);
+            if (xcnt >= 32) flush32<BPL, 2>(xlist, xmask, xcnt, lane, x, y, z, soft2, ax, ay, az);
         }
         apply_entries<BPL, false, false>(list, cnt, x, y, z, soft2, ax, ay, az);
-        apply_masked<BPL>(mlist, mmask, mcnt, lane, x, y, z, soft2, ax, ay, az);
+        apply_masked<BPL, false>(mlist, mmask, mcnt, lane, x, y, z, soft2, ax, ay, az);
+        apply_masked<BPL, true>(xlist, xmask, xcnt, lane, x, y, z, soft2, ax, ay, az);
         __syncwarp();
+        n_inter += n_acc;
+        n_wrap += n_acc;
 #pragma unroll
         for (int b = 0; b < BPL; ++b) {
             if (valid[b]) {
