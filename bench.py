@@ -9,6 +9,11 @@ theta = 0.5, softening 0.5/128, G = 1, kick-drift steps of da = 0.002, and the
 density splat to a 1920x1080 float32 grid with the orbiting 60-degree camera.
 One bench step = one simulation step (63-bit Morton keys, stable sort +
 permute, Karras build, upward pass, force traversal, kick/drift) plus the splat.
+The force traversal is the reference's (physics_kernels.py:14-153) with its
+opening test decided body by body (--mac ref_x): every body gets exactly the
+reference's node set.  The line's "variants" entry times the same loop with
+the test decided once per 64-body bucket (ref_x_bucket: finer node sets, more
+accurate than the reference, not its forces).
 The sort is adaptive (--sort auto): the keys of bodies sorted one step earlier
 mostly keep their order, so a near-sorted path (take out the keys that break the
 order, sort them, merge them back) replaces the full radix sort whenever at most
@@ -48,10 +53,12 @@ N_GRID = 128
 FLOPS_PER_INTERACTION = 20   # 3 sub, 3 min-image, 5 d2, 1 +eps2, 1 rsqrt, 3 mul, 3 fma (+1)
 FULL_SORT_KERNELS = 10     # zeroing + digit histogram + 8 one-sweep passes (63-bit keys)
 E2E_MIN_STEPS = 40         # steps of the end-to-end measurement (at least --steps)
-# DRAM traffic of one k_forces_grouped launch on this workload (64-body buckets, two-level
-# walk), from the ncu capture summarised in profiles/k_forces_grouped_128cube.md
-# (dram__bytes_read.sum + dram__bytes_write.sum)
-FORCES_TRAFFIC_BYTES_128 = 213.2e6 + 21.8e6
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one force-kernel launch on
+# the 128^3 seed-1 workload at theta 0.5 (64-body buckets, two-level walk with 512-body
+# super-buckets), from one ncu capture of each kernel; not measured by this run
+FORCES_TRAFFIC_BYTES_128 = {"ref_x": 209.4e6 + 21.9e6, "ref_x_bucket": 213.2e6 + 21.8e6}
+FORCES_KERNEL = {"ref_x": "k_forces_exact", "ref_x_bucket": "k_forces_grouped",
+                 "periodic": "k_forces_grouped", "ewald": "k_forces_grouped"}
 
 
 def parse():
@@ -233,10 +240,12 @@ def fma_peak_tflops():
 
 # ---------------------------------------------------------------- CPU (reference algorithm)
 
-def cpu_reference_step(pos, vel, mass, a, da, cfg, sample, threads):
+def cpu_reference_step(pos, vel, mass, a, da, cfg, sample, threads, full_check=False):
     """One step of the reference's algorithm on the host (oracle restating
     src/core/engine.py:55-123 with the 63-bit key), forces on `sample`
-    evenly spaced targets scaled to N.  Returns (new pos, new vel, seconds)."""
+    evenly spaced targets scaled to N.  Returns (new pos, new vel, seconds);
+    with `full_check` also a dict comparing the scaled sample with the force
+    traversal timed on every body of the same tree."""
     from oracle import oracle as orc
     n = pos[0].size
     t0 = time.perf_counter()
@@ -259,7 +268,16 @@ def cpu_reference_step(pos, vel, mass, a, da, cfg, sample, threads):
     orc.render_density(*new[:3], mvp, cfg.RES_W, cfg.RES_H)
     t4 = time.perf_counter()
     seconds = (t1 - t0) + (t2 - t1) * n / targets.size + (t4 - t3)
-    return new[:3], new[3:], seconds
+    if not full_check:
+        return new[:3], new[3:], seconds
+    t5 = time.perf_counter()
+    orc.forces_targets_f64(*spos, ch, nm, nc, lo, hi, cfg.THETA, cfg.G, cfg.SOFTENING,
+                           cfg.BOX_SIZE, root, np.arange(n, dtype=np.int64), nthreads=threads)
+    full = time.perf_counter() - t5
+    scaled = (t2 - t1) * n / targets.size
+    check = {"force_targets_sampled": int(targets.size), "force_s_scaled_from_sample": scaled,
+             "force_s_all_bodies_timed": full, "timed_over_scaled": full / scaled}
+    return new[:3], new[3:], seconds, check
 
 
 def run_reference(args):
@@ -276,11 +294,16 @@ def run_reference(args):
     for _ in range(args.warmup):
         cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads)
     total = 0.0
+    wall0 = time.perf_counter()
     for k in range(args.steps):
         pos, vel, s = cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads)
         a += 0.002
         total += s
+    wall = time.perf_counter() - wall0
     value = n * args.steps / total
+    # the sampled force traversal against the traversal timed on every body, once
+    _, _, _, check = cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads,
+                                        full_check=True)
     line = {
         "impl": "reference", "metric": metric_for(args.n_grid), "value": value, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -290,6 +313,11 @@ def run_reference(args):
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
                          "sample": f"all stages on all {n} bodies; force traversal on {args.cpu_sample} "
                                    f"evenly spaced targets scaled to N"},
+        "sampling": {"timed_seconds_actual": wall,
+                     "note": "ms_per_step is the full step the sample stands for: the force traversal "
+                             "of the sampled targets scaled to all bodies (checked below against the "
+                             "traversal timed on every body of one step)",
+                     "check": check},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -429,16 +457,27 @@ def run_ours(args):
     if not args.profile:
         peak = fma_peak_tflops()
         achieved = interactions_per_step * FLOPS_PER_INTERACTION / (forces_ms * 1e-3) / 1e12
-        line["roofline"] = {"kernel": "k_forces_grouped", "bound": "fp32", "achieved": achieved,
+        traffic = FORCES_TRAFFIC_BYTES_128.get(args.mac) if (
+            args.n_grid == 128 and abs(args.theta - 0.5) < 1e-9 and args.force_mode == "grouped") else None
+        line["roofline"] = {"kernel": FORCES_KERNEL.get(args.mac, "k_forces_ref")
+                            if args.force_mode == "grouped" else "k_forces_ref",
+                            "bound": "fp32", "achieved": achieved,
                             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                            "traffic": FORCES_TRAFFIC_BYTES_128 if (args.n_grid == 128 and args.mac == "ref_x"
-                                                                    and abs(args.theta - 0.5) < 1e-9) else None,
-                            "traffic_unit": "bytes per launch (ncu capture, profiles/k_forces_grouped_128cube.md)",
+                            "traffic": traffic,
+                            "traffic_unit": "bytes per launch",
+                            "traffic_source": "ncu capture of this kernel on this workload (one launch, "
+                                              "64-body buckets, 512-body super-buckets), not this run"
+                                              if traffic else None,
                             "note": "peak = measured FP32 FMA throughput (cnb_fma_probe); "
-                                    f"{FLOPS_PER_INTERACTION} flops per body-node interaction"}
+                                    f"{FLOPS_PER_INTERACTION} flops per body-node interaction; "
+                                    "interactions = the accepted (body, node) pairs counted on the device"}
         line["clocks"] = sampler.summary()
         line["accuracy"] = accuracy(eng, args)
         line["e2e"] = e2e(eng, args, ws)
+        if args.mac == "ref_x" and args.force_mode == "grouped":
+            # the reference's test decided once per bucket: finer node sets than the
+            # reference's (not its forces), reported beside the headline
+            line["variants"] = [variant(eng, args, "ref_x_bucket", flush)]
         if rank == 0:
             line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
@@ -447,6 +486,43 @@ def run_ours(args):
         import torch.distributed as dist
         dist.destroy_process_group()
     return 0
+
+
+def variant(eng, args, mac_name, flush):
+    """The timed loop of the headline (CUDA-graph replays of two steps with
+    splats, L2 flushed between replays) with another opening test, plus its
+    interaction count and force error; the engine keeps its launch shape."""
+    import torch
+    from cnb.core.engine import MACS
+    saved = eng.mac
+    eng.mac = MACS[mac_name]
+    try:
+        eng.stats.zero_()
+        eng.enable_stage_timing(True)
+        for _ in range(2):
+            eng.step()
+        stages = {k: v / 2 for k, v in eng.stage_times().items()}
+        eng.enable_stage_timing(False)
+        inter = float(eng.stats[0].item()) / 2 / eng.state.n
+        eng.capture(splat=True)
+        reps = 5
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+        for k in range(reps):
+            flush.zero_()
+            starts[k].record()
+            eng.replay()
+            ends[k].record()
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / (2 * reps)
+        eng.check()
+        acc = accuracy(eng, args)
+    finally:
+        eng.mac = saved
+        eng._graph = None
+    return {"mac": mac_name, "value": eng.state.n / (ms * 1e-3), "unit": "particle-steps/s",
+            "ms_per_step": ms, "steps": 2 * reps, "forces_ms_eager": stages.get("forces"),
+            "interactions_per_body": inter, "accuracy": acc}
 
 
 def accuracy(eng, args):
