@@ -148,3 +148,17 @@ def test_direct_sum_antisymmetry():
     acc = orc.direct_sum(x, y, z, mass, np.arange(n), 1.0, 0.01)
     # equal masses: total momentum change is zero (pairwise antisymmetric law)
     assert np.abs(acc.sum(axis=0)).max() < 1e-9 * np.abs(acc).max()
+
+
+
+def test_mvp_matches_reference(golden_files):
+    """cnb.utils.visualizer.get_mvp_matrix at the reference's square aspect
+    equals the matrix the reference's own get_mvp_matrix produced
+    (src/utils/visualizer.py:81-112, recorded in each fixture by
+    make_golden.py for step 3, centre (0.5, 0.5, 0.5), box 1)."""
+    from cnb.utils import config as cfgmod
+    from cnb.utils.visualizer import get_mvp_matrix
+    got = get_mvp_matrix(3, (0.5, 0.5, 0.5), 1.0, cfgmod.make())
+    assert got.dtype == np.float32
+    for f in golden_files:
+        np.testing.assert_array_equal(got, _load(f)["mvp"])
