@@ -92,8 +92,8 @@ SIGNATURES = {
     "cnb_forces_grouped_boxes": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p, _int, _p, _p, _p, _int, _int,
                                         _int, _d, _p, _p, _p]),
     "cnb_integrate_boxes": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _int, _i64, _p, _p]),
-    "cnb_bucket_features": (_int, [_p, _p, _p, _i64, _p, _int, _p]),
-    "cnb_controller_theta": (_int, [_p, _p, _p, _i64, _p, _p, _int, _p]),
+    "cnb_bucket_features": (_int, [_p, _p, _p, _i64, _p, _p, _p, _int, _p]),
+    "cnb_controller_theta": (_int, [_p, _p, _p, _i64, _p, _p, _p, _p, _int, _p]),
     "cnb_mlp_predict": (_int, [_p, _int, _p, _p, _p]),
     "cnb_mlp_grad": (_int, [_p, _p, _int, _p, _f, _p, _p, _p, _p]),
     "cnb_adam_step": (_int, [_p, _p, _p, _p, _int, _f, _f, _f, _f, _int, _p]),
@@ -101,12 +101,12 @@ SIGNATURES = {
     "cnb_colorize": (_int, [_p, _int, _int, _p, _p, _p, _p]),
     "cnb_ewald_table": (_int, [_p, _int, _p]),
     "cnb_forces_grouped_ewald": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _d, _d, _p,
-                                        _int, _p, _p, _p, _p]),
+                                        _int, _p, _p, _p, _p, _p]),
     "cnb_upward_table_quad": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_upward_table_buckets": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_direct_sum_ewald_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_forces_grouped_boxes_ewald": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p, _int, _p, _p, _p, _int,
-                                              _int, _d, _p, _int, _p, _p, _p]),
+                                              _int, _d, _p, _int, _p, _p, _p, _p]),
     "cnb_direct_sum_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_fma_probe": (_int, [_p, _i64, _int, _p]),
 }

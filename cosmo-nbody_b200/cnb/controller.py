@@ -8,8 +8,9 @@ and the training kernels (forward/backward, parameter gradients, Adam).
 
 Training pairs come from the batched boxes (cnb.core.batched): for sampled
 buckets the plain fixed-theta traversal is run at every theta of a grid and
-compared with the float64 direct sum; a bucket's label is the largest theta
-whose error stays within the budget.  Plain fixed-theta Barnes-Hut remains
+compared with the float64 direct sum; the labels are the per-bucket angles
+that minimise the interactions while the global error percentile stays at
+plain theta = 0.5's (allocate()).  Plain fixed-theta Barnes-Hut remains
 the fallback (no weights: theta_per_bucket = None) and the reference for the
 error budget.
 """
@@ -114,15 +115,19 @@ class ThetaController:
         _lib.call("cnb_to_bf16", p.data_ptr(), self.weights_bf16.data_ptr(), N_PARAMS, _st())
         return self.weights_bf16
 
-    def theta_for_buckets(self, node_table, parents, workspace, n, out=None, scale=1.0):
-        """theta per bucket slot of a built tree (fused features + network)."""
+    def theta_for_buckets(self, node_table, parents, workspace, n, accel, perm=None, out=None,
+                          scale=1.0):
+        """theta per bucket slot of a built tree (fused features + network);
+        accel: the previous step's accelerations [N, 3], perm: row of accel
+        for each body of the sorted order (None: the same order)."""
         if self.weights_bf16 is None:
             self.export()
         max_b = (workspace.numel() - 4) // 4
         if out is None:
             out = torch.empty(max_b, dtype=torch.float32, device=self.device)
         _lib.call("cnb_controller_theta", node_table.data_ptr(), parents.data_ptr(),
-                  workspace.data_ptr(), n, self.weights_bf16.data_ptr(), out.data_ptr(), max_b, _st())
+                  workspace.data_ptr(), n, accel.data_ptr(), perm.data_ptr() if perm is not None else None,
+                  self.weights_bf16.data_ptr(), out.data_ptr(), max_b, _st())
         if scale != 1.0:
             out.mul_(scale).clamp_(0.2, 1.0)
         return out
@@ -140,11 +145,12 @@ class ThetaController:
         return self
 
 
-def bucket_features(node_table, parents, workspace, n):
+def bucket_features(node_table, parents, workspace, n, accel, perm=None):
     max_b = (workspace.numel() - 4) // 4
     out = torch.empty((max_b, N_IN), dtype=torch.float32, device=node_table.device)
     _lib.call("cnb_bucket_features", node_table.data_ptr(), parents.data_ptr(), workspace.data_ptr(),
-              n, out.data_ptr(), max_b, _st())
+              n, accel.data_ptr(), perm.data_ptr() if perm is not None else None, out.data_ptr(),
+              max_b, _st())
     nb = int(workspace[0].item())
     return out[:nb]
 
@@ -160,23 +166,88 @@ def direct_sum(pos, mass, targets, G, soft, periodic=False):
     return out
 
 
+def allocate(errors, costs, owner, budget, allowed):
+    """Per-bucket choice of theta minimising the total cost subject to at most
+    `allowed` bodies with an error above `budget` (the global-quantile
+    constraint of the metric, not a per-bucket one).
+
+    errors [T, n_bodies] per theta of the grid, costs [T, n_buckets] (body
+    interactions of each bucket at each theta), owner [n_bodies] the bucket
+    of each body.  Lagrangian relaxation: for a price lam per violating body
+    every bucket picks the theta minimising cost + lam * violations; lam is
+    bisected to the smallest price whose choice meets `allowed`.  Returns
+    (index of the chosen theta per bucket, total cost, violations)."""
+    errors = np.asarray(errors, np.float64)
+    costs = np.asarray(costs, np.float64)
+    T, G = costs.shape
+    viol = np.zeros((T, G))
+    for k in range(T):
+        np.add.at(viol[k], owner, errors[k] > budget)
+
+    def pick(lam):
+        idx = np.argmin(costs + lam * viol, axis=0)
+        return idx, viol[idx, np.arange(G)].sum()
+
+    # with an unbounded price every bucket minimises its violations first
+    big = costs.max() * (G + 1) + 1.0
+    idx_big, v_big = pick(big)
+    if v_big > allowed:
+        return idx_big, float(costs[idx_big, np.arange(G)].sum()), float(v_big)
+    lo, hi = 0.0, big
+    idx_lo, v_lo = pick(lo)
+    if v_lo <= allowed:
+        return idx_lo, float(costs[idx_lo, np.arange(G)].sum()), float(v_lo)
+    for _ in range(100):
+        mid = 0.5 * (lo + hi)
+        _, v = pick(mid)
+        if v <= allowed:
+            hi = mid
+        else:
+            lo = mid
+    idx, v = pick(hi)
+    return idx, float(costs[idx, np.arange(G)].sum()), float(v)
+
+
+def _per_body_errors(got, ref, refn):
+    return ((got.double() - ref).norm(dim=1) / refn).cpu().numpy()
+
+
 def make_labels(bb: BatchedBoxes, theta_grid=THETA_GRID, budget=None, per_box=48, seed=0,
-                error="rms"):
+                error="relative", objective=None, quantile=99.0):
     """(features, labels, info) for sampled buckets of every box of `bb`.
 
-    For every theta of the grid the plain traversal runs with that theta in
-    every bucket; each sampled bucket's error is the largest force error of
-    its bodies against the float64 direct sum of its box (under the box's
-    force law: minimum image, or periodic for the "ewald" test), either relative to
+    For every theta of the grid the traversal runs with that theta in every
+    bucket (a body's force depends only on its own bucket's theta); each
+    sampled bucket's bodies are compared with the float64 direct sum of
+    their box (minimum image, or periodic for the "ewald" test), relative to
     the body's own acceleration (error="relative") or to the box's RMS
-    acceleration (error="rms").  The label is the largest theta whose error
-    is within `budget`; budget None means the 99th-percentile error of plain
-    theta = 0.5 over all sampled bodies.  Buckets that miss the budget even at
-    the smallest theta get the smallest theta (counted in info["saturated"])."""
+    acceleration (error="rms").  `budget` None: the `quantile`-th percentile
+    error of plain theta = 0.5 over all sampled bodies.
+
+    objective "lagrangian" (default under the periodic law, which reports
+    per-bucket costs): the labels are the per-bucket angles that minimise the
+    sampled buckets' total interactions while no more bodies exceed the
+    budget than under plain theta = 0.5 -- the metric's own constraint (a
+    global percentile), found by allocate(); info["bound"] is that
+    allocation's cost ratio against plain theta = 0.5, an upper bound for any
+    per-bucket policy on these buckets.  objective "worst": the largest theta
+    whose worst body stays within the budget (a stricter, per-bucket rule).
+
+    The features' acceleration input is the plain theta = 0.5 force of the
+    same state (the previous step's force in a running simulation)."""
     rng = np.random.default_rng(seed)
+    periodic = bb.mac == _lib.MAC_EWALD
+    if objective is None:
+        objective = "lagrangian" if periodic else "worst"
+    if objective == "lagrangian" and not periodic:
+        raise ValueError("per-bucket costs are recorded under the periodic (Ewald) law only")
     bb.sort_and_build()
-    feats = bucket_features(bb.table, bb.parent, bb.workspace, bb.n)
     bk = bb.buckets().cpu().numpy()
+    nb = bk.shape[0]
+    tpb = torch.full((max(nb, 1),), 0.5, dtype=torch.float32, device=bb.device)
+    bb.compute_forces(theta_per_bucket=tpb)
+    accel = bb.force.clone()
+    feats = bucket_features(bb.table, bb.parent, bb.workspace, bb.n, accel)
     box_of = np.searchsorted(bb.offsets, bk[:, 0], side="right") - 1
     chosen = []
     for b in range(bb.n_boxes):
@@ -196,7 +267,7 @@ def make_labels(bb: BatchedBoxes, theta_grid=THETA_GRID, budget=None, per_box=48
         local = torch.from_numpy(t - sl.start).to(bb.device)
         soft = 0.5 / bb.boxes[b]["n_grid"]
         ref.append(direct_sum([p[sl] for p in bb.pos], bb.mass[sl], local, bb.G, soft,
-                              periodic=bb.mac == _lib.MAC_EWALD))
+                              periodic=periodic))
         bodies.append(t)
         owner.append(o)
     box_rms = [r.norm(dim=1).pow(2).mean().sqrt().expand(r.shape[0]) for r in ref]
@@ -204,26 +275,40 @@ def make_labels(bb: BatchedBoxes, theta_grid=THETA_GRID, budget=None, per_box=48
     owner = np.concatenate(owner)
     ref = torch.cat(ref)
     refn = ref.norm(dim=1) if error == "relative" else torch.cat(box_rms)
-    errs = np.zeros((len(theta_grid), chosen.size))
-    body_err = {}
-    nb = bk.shape[0]
+    T = len(theta_grid)
+    body_err = np.zeros((T, bodies.numel()))
+    costs = np.zeros((T, chosen.size))
+    counts = bk[chosen, 1].astype(np.float64)
+    inter = torch.zeros(max(nb, 1), dtype=torch.int32, device=bb.device)
     cost = []
     for k, th in enumerate(theta_grid):
         tpb = torch.full((max(nb, 1),), float(th), dtype=torch.float32, device=bb.device)
         bb.stats.zero_()
-        bb.compute_forces(theta_per_bucket=tpb)
-        e = ((bb.force[bodies].double() - ref).norm(dim=1) / refn).cpu().numpy()
-        body_err[th] = e
-        np.maximum.at(errs[k], owner, e)
+        bb.compute_forces(theta_per_bucket=tpb, bucket_inter=inter if periodic else None)
+        body_err[k] = _per_body_errors(bb.force[bodies], ref, refn)
+        if periodic:
+            costs[k] = inter[torch.from_numpy(chosen).to(bb.device)].cpu().numpy() * counts
         cost.append(float(bb.stats[0].item()) / bb.n)
     bb.check()
+    k05 = theta_grid.index(0.5)
     if budget is None:
-        budget = float(np.percentile(body_err[0.5], 99))
-    ok = errs <= budget
-    labels = np.full(chosen.size, theta_grid[0], np.float32)
-    for k, th in enumerate(theta_grid):
-        labels[ok[k]] = th      # ascending grid: the largest passing theta wins
-    info = dict(budget=budget, saturated=float(np.mean(~ok.any(axis=0))), cost_per_theta=cost,
-                n_samples=int(chosen.size), label_hist=np.bincount(
-                    np.searchsorted(theta_grid, labels), minlength=len(theta_grid)).tolist())
+        budget = float(np.percentile(body_err[k05], quantile))
+    info = dict(budget=budget, error=error, objective=objective, cost_per_theta=cost,
+                n_samples=int(chosen.size), n_bodies=int(bodies.numel()))
+    if objective == "lagrangian":
+        allowed = int((body_err[k05] > budget).sum())
+        idx, total, v = allocate(body_err, costs, owner, budget, allowed)
+        labels = np.asarray(theta_grid, np.float32)[idx]
+        plain_cost = costs[k05].sum()
+        info.update(allowed_violations=allowed, violations=v, bound=float(plain_cost / total))
+    else:
+        errs = np.zeros((T, chosen.size))
+        for k in range(T):
+            np.maximum.at(errs[k], owner, body_err[k])
+        ok = errs <= budget
+        labels = np.full(chosen.size, theta_grid[0], np.float32)
+        for k, th in enumerate(theta_grid):
+            labels[ok[k]] = th      # ascending grid: the largest passing theta wins
+        info["saturated"] = float(np.mean(~ok.any(axis=0)))
+    info["label_hist"] = np.bincount(np.searchsorted(theta_grid, labels), minlength=T).tolist()
     return feats[torch.from_numpy(chosen).to(bb.device)], torch.from_numpy(labels).to(bb.device), info

@@ -158,7 +158,9 @@ class BatchedBoxes:
                   self.codes_sorted.data_ptr(), self.box_bits, n, self.n_boxes,
                   self.box_roots.data_ptr(), st)
 
-    def compute_forces(self, theta_per_bucket=None):
+    def compute_forces(self, theta_per_bucket=None, bucket_inter=None):
+        """Forces of every box; `bucket_inter` (device int32 per bucket slot,
+        periodic law only) receives each bucket's interactions per body."""
         st = self._st()
         tpb = theta_per_bucket if theta_per_bucket is not None else self.theta_per_bucket
         p = self.pos
@@ -168,8 +170,9 @@ class BatchedBoxes:
                       self.force.data_ptr(), self.n, self.codes_sorted.data_ptr(), self.box_bits,
                       self.box_roots.data_ptr(), self.box_params.data_ptr(),
                       tpb.data_ptr() if tpb is not None else None, self.bpl, self.block_warps, self.G,
-                      self.ewald_table.data_ptr(), EWALD_NT, self.stats.data_ptr(),
-                      status_buffer(self.device.index).data_ptr(), st)
+                      self.ewald_table.data_ptr(), EWALD_NT,
+                      bucket_inter.data_ptr() if bucket_inter is not None else None,
+                      self.stats.data_ptr(), status_buffer(self.device.index).data_ptr(), st)
             return
         _lib.call("cnb_forces_grouped_boxes", p[0].data_ptr(), p[1].data_ptr(), p[2].data_ptr(),
                   self.table.data_ptr(), self.workspace.data_ptr(), self.force.data_ptr(), self.n,

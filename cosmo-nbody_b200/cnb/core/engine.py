@@ -66,6 +66,15 @@ class SimulationEngine:
         # learned opening-angle controller (cnb.controller.ThetaController); None = plain theta
         self.controller = None
         self.controller_scale = 1.0
+        # periodic law: device int32 per bucket slot receiving each bucket's
+        # interactions per body (None: not recorded)
+        self.bucket_inter = None
+        # the controller's acceleration input: None = the previous step's forces
+        # (state.force); a tensor [N, 3] in the current sorted order overrides it
+        self.controller_accel = None
+        # True while state.force holds forces in the current sorted order (a
+        # sort since the last force stage leaves it in the previous order)
+        self._force_current = False
         self.stats = torch.zeros(4, dtype=torch.int64, device=state.device)
         self.mac = MACS[getattr(config, "MAC", "ref_x")]
         # periodic test: image-ambiguous nodes of at most SLAB_BODIES bodies' mass are applied
@@ -110,6 +119,10 @@ class SimulationEngine:
 
     def compute_forces(self):
         """The force stage of engine.py:91-111, one launch over all bodies."""
+        self._compute_forces()
+        self._force_current = True
+
+    def _compute_forces(self):
         cfg, s, tm = self.config, self.state, self.tree_manager
         st = self._stream()
         status = status_buffer(s.device.index).data_ptr()
@@ -117,9 +130,14 @@ class SimulationEngine:
         if self.force_mode == "grouped":
             if self.controller is not None:
                 # learned per-bucket theta (fused features + network on the GPU)
+                # the previous step's accelerations, row s.perm[i] for the body now at i
+                if self.controller_accel is not None:
+                    accel, perm = self.controller_accel, None
+                else:
+                    accel, perm = s.force, (None if self._force_current else s.perm)
                 self.theta_per_group = self.controller.theta_for_buckets(
-                    tm.node_table, tm.parent, tm.workspace, s.n, out=self.theta_per_group,
-                    scale=self.controller_scale)
+                    tm.node_table, tm.parent, tm.workspace, s.n, accel, perm,
+                    out=self.theta_per_group, scale=self.controller_scale)
             tpg = self.theta_per_group
             if self.ewald_table is not None:
                 _lib.call("cnb_forces_grouped_ewald", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
@@ -128,6 +146,7 @@ class SimulationEngine:
                           self.bodies_per_lane, self.block_warps, float(cfg.G), float(cfg.SOFTENING),
                           self.ewald_table.data_ptr(), EWALD_NT,
                           tm.quad.data_ptr() if tm.quad is not None else None,
+                          self.bucket_inter.data_ptr() if self.bucket_inter is not None else None,
                           self.stats.data_ptr(), status, st)
                 return
             if self.super_ws is not None and tpg is None:
@@ -171,6 +190,7 @@ class SimulationEngine:
         """Sort, tree and forces for the current state (no integration)."""
         self._mark("start")
         self.state.sort_buffer_by_morton(self.config)
+        self._force_current = False
         self._mark("sort")
         self.tree_manager.build(self.state.pos, self.state.mass, self.state.codes)
         self._mark("tree")

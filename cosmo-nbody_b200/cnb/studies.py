@@ -2,7 +2,7 @@
 
     python -m cnb.studies precision   [--n-grid 256] [--steps 50]
     python -m cnb.studies batched     [--boxes 64] [--steps 10]
-    python -m cnb.studies controller  [--n-grid 128] [--evolve 100] [--mac ewald]
+    python -m cnb.studies controller  [--n-grid 128] [--evolve 100] [--save weights.npz]
     python -m cnb.studies multipole   [--n-grid 128] [--evolve 100]
 
 precision:  Zel'dovich n^3 (seed 2) evolved `steps` kick-drift steps from
@@ -15,11 +15,12 @@ batched:    64 boxes, n drawn from {16, 24, 32, 48, 64}^3 (seed 3), a_start in
             [0.02, 0.1], theta in [0.3, 0.8]: particle-steps/s of the batched
             step (one persistent traversal launch, CUDA graph) against the
             same boxes stepped one by one.
-controller: labels from the batched boxes, training on the GPU, and learned
-            theta against plain theta = 0.5 at matched 99th-percentile error
-            on an evolved n^3 state (seed 4); under the minimum-image law with
-            the exact periodic test (default), or with --mac ewald under the
-            periodic (Ewald) law, each against its own float64 direct sum.
+controller: under the periodic (Ewald) law: labels from the batched boxes
+            (the per-bucket angles of least cost at plain theta = 0.5's global
+            p99), training on the GPU, the same allocation computed on every
+            bucket of an evolved n^3 state (seed 4) as the bound of any
+            per-bucket policy, and learned theta against plain theta = 0.5 at
+            matched p99 relative error there.
 multipole:  under the periodic law on the same evolved state: monopoles at
             theta = 0.5 against quadrupoles over a theta grid (p99 error
             against the float64 Ewald direct sum, interactions, forces ms).
@@ -210,30 +211,89 @@ def batched(args):
                           speedup=seq_ms / batched_ms)), flush=True)
 
 
+def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
+    """The cheapest per-bucket allocation of theta on the engine's current
+    tree at the same global error percentile as plain theta = 0.5: every
+    bucket of the state, per-body errors relative to `ref` (accelerations
+    [N, 3] in the current sorted order, float64), costs from the kernel's
+    per-bucket interaction counts, allocate() for the choice.  Returns a dict
+    with the bound (plain cost / allocated cost) and the chosen angles."""
+    from .controller import THETA_GRID, allocate
+    thetas = THETA_GRID if thetas is None else thetas
+    tm, s = eng.tree_manager, eng.state
+    nb = int(tm.workspace[0].item())
+    bk = tm.workspace[4:4 + 4 * nb].view(-1, 4).cpu().numpy()
+    owner = np.repeat(np.arange(nb), bk[:, 1])
+    order = np.concatenate([np.arange(b[0], b[0] + b[1]) for b in bk])
+    refn = ref.norm(dim=1)
+    inter = torch.zeros(max(nb, 1), dtype=torch.int32, device=s.pos[0].device)
+    eng.bucket_inter = inter
+    errs = np.zeros((len(thetas), s.n))
+    costs = np.zeros((len(thetas), nb))
+    saved = eng.theta_per_group, eng.controller
+    eng.controller = None
+    try:
+        for k, th in enumerate(thetas):
+            eng.theta_per_group = torch.full((nb,), float(th), device=s.pos[0].device)
+            eng.compute_forces()
+            e = ((s.force.double() - ref).norm(dim=1) / refn).cpu().numpy()
+            errs[k] = e[order]
+            costs[k] = inter[:nb].cpu().numpy().astype(np.float64) * bk[:, 1]
+    finally:
+        eng.bucket_inter = None
+        eng.theta_per_group, eng.controller = saved
+    k05 = list(thetas).index(0.5)
+    budget = float(np.percentile(errs[k05], quantile))
+    allowed = int((errs[k05] > budget).sum())
+    idx, total, v = allocate(errs, costs, owner, budget, allowed)
+    chosen = np.asarray(thetas)[idx]
+    return dict(bound=float(costs[k05].sum() / total), budget_rel=budget, allowed=allowed,
+                violations=v, buckets=nb,
+                theta_hist={f"{t:.1f}": int((chosen == t).sum()) for t in thetas},
+                interactions_per_body_plain=float(costs[k05].sum() / s.n),
+                interactions_per_body_bound=float(total / s.n))
+
+
 def controller(args):
+    """Learned theta under the periodic (Ewald) law: labels from the 64
+    batched boxes (Lagrangian allocation at plain theta = 0.5's global p99),
+    training on the GPU, the bound of any per-bucket policy on the evolved
+    128^3 state, and the trained network against plain theta = 0.5 there at
+    matched p99 (relative error; against a reference-accuracy tree on every
+    body and against the float64 Ewald direct sum on a sample)."""
     from .controller import ThetaController, make_labels
     t0 = time.time()
-    law = "ewald" if args.mac == "ewald" else "periodic"
-    train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac=law, bodies_per_lane=args.bpl)
-    X, y, info = make_labels(train, per_box=args.per_box, error=args.error)
+    train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac="ewald", bodies_per_lane=args.bpl)
+    X, y, info = make_labels(train, per_box=args.per_box, error="relative")
     del train
     ctl = ThetaController(seed=0)
-    curve = ctl.train(X, y, steps=args.train_steps, lr=3e-3, over_weight=4.0)
+    curve = ctl.train(X, y, steps=args.train_steps, lr=3e-3, over_weight=args.over_weight)
+    if args.save:
+        ctl.save(args.save)
+    t_train = time.time() - t0
     pos, vel, a = _evolve(args.n_grid, 4, args.evolve)
     n = args.n_grid ** 3
-    cfg = _cfg(args.n_grid, MAC=law, BODIES_PER_LANE=args.bpl)
-    st = SimulationState(n, pos, vel)
-    eng = SimulationEngine(cfg, st, camera=False)
+    eng = SimulationEngine(_cfg(args.n_grid, MAC="ewald", BODIES_PER_LANE=args.bpl, BLOCK_WARPS=4),
+                           SimulationState(n, pos, vel), camera=False)
     eng.forces_only()
-    # the periodic oracle costs hundreds of float64 terms per pair: fewer targets
-    n_t = 4096 if law == "periodic" else 1024
-    targets = np.sort(np.random.default_rng(0).choice(n, n_t, replace=False)).astype(np.int64)
-    ref = _direct(st, targets, cfg.SOFTENING, periodic=law == "ewald")
-    key = "p99_rms" if args.error == "rms" else "p99_rel"
+    plain_acc = eng.state.force.clone()
+    # reference-accuracy forces on every body: quadrupoles at theta = 0.2 (same sort)
+    qeng = SimulationEngine(_cfg(args.n_grid, MAC="ewald", QUADRUPOLE=True, THETA=0.2,
+                                 BODIES_PER_LANE=args.bpl, BLOCK_WARPS=4),
+                            SimulationState(n, pos, vel), camera=False)
+    qeng.forces_only()
+    ref_tree = qeng.state.force.double()
+    targets = np.sort(np.random.default_rng(0).choice(n, args.sample, replace=False)).astype(np.int64)
+    ref_direct = _direct(eng.state, targets, eng.config.SOFTENING, periodic=True)
+    tree_err = _errors(qeng.state.force, ref_direct, targets)
+    del qeng
+    bound = lagrangian_bound(eng, ref_tree)
+    T = torch.from_numpy(targets).cuda()
 
     def run(scale=None):
         eng.controller = ctl if scale is not None else None
         eng.controller_scale = scale or 1.0
+        eng.controller_accel = plain_acc
         if scale is None:
             eng.theta_per_group = None
         eng.stats.zero_()
@@ -242,23 +302,30 @@ def controller(args):
         eng.compute_forces()
         e1.record()
         torch.cuda.synchronize()
-        s = eng.stats.cpu().numpy()
-        return dict(_errors(st.force, ref, targets), ms=e0.elapsed_time(e1),
-                    interactions=float(s[0]) / n, theta_dependent=float(s[0] - s[2]) / n)
+        st = eng.state
+        e_all = ((st.force.double() - ref_tree).norm(dim=1) / ref_tree.norm(dim=1))
+        return dict(_errors(st.force, ref_direct, targets), ms=e0.elapsed_time(e1),
+                    p99_rel_all_vs_tree=float(torch.quantile(e_all.float(), 0.99).item()),
+                    interactions=float(eng.stats[0].item()) / n)
 
     plain = run(None)
-    lo, hi = 0.3, 3.0
-    for _ in range(12):
+    key = "p99_rel_all_vs_tree"
+    lo, hi = 0.2, 3.0
+    for _ in range(14):
         mid = 0.5 * (lo + hi)
         r = run(mid)
         lo, hi = (mid, hi) if r[key] <= plain[key] else (lo, mid)
     learned = run(lo)
     eng.controller = None
+    eng.controller_accel = None
     eng.check()
-    print(json.dumps(dict(study="controller", law=law, n_grid=args.n_grid, evolve_steps=args.evolve, a=a,
-                          error=args.error, labels=info, train_loss=[curve[0], curve[-1]],
+    gain = plain["interactions"] / learned["interactions"]
+    print(json.dumps(dict(study="controller", law="ewald", n_grid=args.n_grid, evolve_steps=args.evolve,
+                          a=a, labels=info, train_loss=[curve[0], curve[-1]], train_seconds=t_train,
+                          reference_tree_vs_direct=tree_err, bound=bound,
                           plain_theta05=plain, learned=learned, learned_scale=lo,
-                          speedup_forces=plain["ms"] / learned["ms"],
+                          gain_interactions=gain, gain_forces_ms=plain["ms"] / learned["ms"],
+                          fraction_of_bound=gain / bound["bound"],
                           seconds=time.time() - t0)), flush=True)
 
 
@@ -313,7 +380,11 @@ def main():
     ap.add_argument("--evolve", type=int, default=100)
     ap.add_argument("--per-box", type=int, default=48)
     ap.add_argument("--train-steps", type=int, default=1500)
-    ap.add_argument("--error", default="rms", choices=["rms", "relative"])
+    ap.add_argument("--error", default="relative", choices=["rms", "relative"])
+    ap.add_argument("--sample", type=int, default=1024, help="direct-sum sample of the controller study")
+    ap.add_argument("--over-weight", type=float, default=4.0,
+                    help="controller training: weight of over-estimated theta in the loss")
+    ap.add_argument("--save", default=None, help="controller study: write the trained weights here")
     ap.add_argument("--bpl", type=int, default=1, choices=[1, 2])
     args = ap.parse_args()
     if args.study == "precision":

@@ -11,7 +11,11 @@
 //
 // Features of a bucket (its subtree node v, ancestors p1..p3), lengths in
 // units of the box's mean body spacing s = (body mass)^(1/3):
-//   f0  log2(extent(v) / s)                f1  log2(bodies) / 5
+//   f0  log2(extent(v) / s)
+//   f1  log2(mean |a| of the bucket's bodies at the previous step over
+//       G mass(p3) / extent(p3)^2, the force scale of the third ancestor)
+//       / 4: the relative force error a given theta leaves grows as the
+//       bucket's own acceleration shrinks
 //   f2  log2(density(v) / mean density)
 //   f3+3k..f5+3k (k = 0..2, ancestor p_{k+1}):
 //       log2(extent(p) / extent(v)), log2(mass(p) / mass(v)),
@@ -38,7 +42,8 @@ __device__ __forceinline__ float node_extent(const float4 *aabb, int v) {
 }
 
 __device__ void bucket_features(const float4 *__restrict__ rec, const float4 *__restrict__ aabb,
-                                const int32_t *__restrict__ parents, int4 bk, float f[kIn]) {
+                                const int32_t *__restrict__ parents, const float *__restrict__ accel,
+                                const uint32_t *__restrict__ perm, int4 bk, float f[kIn]) {
     const int v = bk.z;
     const float4 A = rec[2 * v];
     const float m_body = A.w / (float)bk.y;
@@ -47,31 +52,44 @@ __device__ void bucket_features(const float4 *__restrict__ rec, const float4 *__
     const float ext = fmaxf(node_extent(aabb, v), 1e-3f * s);
     const float vol = (hi.x - lo.x + s) * (hi.y - lo.y + s) * (hi.z - lo.z + s);
     f[0] = __log2f(ext / s);
-    f[1] = __log2f((float)bk.y) * 0.2f;
     f[2] = __log2f((float)bk.y * s * s * s / vol);
     int p = v;
+    float pe = ext, pm = A.w;
     for (int k = 0; k < 3; ++k) {
         const int q = parents[p];
         if (q >= 0) p = q;
         const float4 P = rec[2 * p];
-        const float pe = fmaxf(node_extent(aabb, p), ext);
+        pe = fmaxf(node_extent(aabb, p), ext);
+        pm = fmaxf(P.w, A.w);
         const float dx = P.x - A.x, dy = P.y - A.y, dz = P.z - A.z;
         f[3 + 3 * k] = __log2f(pe / ext);
-        f[4 + 3 * k] = __log2f(fmaxf(P.w, A.w) / A.w);
+        f[4 + 3 * k] = __log2f(pm / A.w);
         f[5 + 3 * k] = sqrtf(dx * dx + dy * dy + dz * dz) / pe;
     }
+    float amean = 0.f;
+    for (int k = 0; k < bk.y; ++k) {
+        const int64_t i = (int64_t)bk.x + k;
+        const int64_t r = perm ? (int64_t)perm[i] : i;
+        const float ax = accel[3 * r], ay = accel[3 * r + 1], az = accel[3 * r + 2];
+        amean += sqrtf(ax * ax + ay * ay + az * az);
+    }
+    amean /= (float)bk.y;
+    // G = 1 in the box's units: the scale is the third ancestor's M / l^2
+    f[1] = 0.25f * __log2f(fmaxf(amean * pe * pe / pm, 1e-6f));
 }
 
 __global__ void __launch_bounds__(256) k_features(const float4 *__restrict__ rec,
                                                   const float4 *__restrict__ aabb,
                                                   const int32_t *__restrict__ parents,
                                                   const int32_t *__restrict__ ws,
+                                                  const float *__restrict__ accel,
+                                                  const uint32_t *__restrict__ perm,
                                                   float *__restrict__ out, int max_buckets) {
     const int nb = min(ws[0], max_buckets);
     const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
         float f[kIn];
-        bucket_features(rec, aabb, parents, buckets[g], f);
+        bucket_features(rec, aabb, parents, accel, perm, buckets[g], f);
 #pragma unroll
         for (int k = 0; k < kIn; ++k) out[(int64_t)g * kIn + k] = f[k];
     }
@@ -109,6 +127,8 @@ __global__ void __launch_bounds__(256) k_controller(const float4 *__restrict__ r
                                                     const float4 *__restrict__ aabb,
                                                     const int32_t *__restrict__ parents,
                                                     const int32_t *__restrict__ ws,
+                                                    const float *__restrict__ accel,
+                                                    const uint32_t *__restrict__ perm,
                                                     const __nv_bfloat16 *__restrict__ wbf,
                                                     float *__restrict__ theta, int max_buckets) {
     __shared__ float w[kParams];
@@ -118,7 +138,7 @@ __global__ void __launch_bounds__(256) k_controller(const float4 *__restrict__ r
     const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
         float f[kIn];
-        bucket_features(rec, aabb, parents, buckets[g], f);
+        bucket_features(rec, aabb, parents, accel, perm, buckets[g], f);
         theta[g] = theta_of(mlp_forward(w, f));
     }
 }
@@ -285,28 +305,29 @@ __global__ void k_to_bf16(const float *__restrict__ src, __nv_bfloat16 *__restri
 using namespace cnb;
 
 extern "C" int cnb_bucket_features(const float *node_table, const int32_t *parents,
-                                   const int32_t *workspace, int64_t n, float *features,
-                                   int max_buckets, void *stream) {
-    if (n < 1 || !node_table || !parents || !workspace || !features || max_buckets < 0)
+                                   const int32_t *workspace, int64_t n, const float *accel,
+                                   const uint32_t *perm, float *features, int max_buckets,
+                                   void *stream) {
+    if (n < 1 || !node_table || !parents || !workspace || !accel || !features || max_buckets < 0)
         return CNB_E_INVALID_ARG;
     const int64_t m = 2 * n - 1;
     const float4 *rec = reinterpret_cast<const float4 *>(node_table);
     k_features<<<grid_for(max_buckets, 256), 256, 0, as_stream(stream)>>>(
-        rec, rec + 2 * m, parents, workspace, features, max_buckets);
+        rec, rec + 2 * m, parents, workspace, accel, perm, features, max_buckets);
     return launch_status();
 }
 
 extern "C" int cnb_controller_theta(const float *node_table, const int32_t *parents,
-                                    const int32_t *workspace, int64_t n,
-                                    const void *weights_bf16, float *theta, int max_buckets,
-                                    void *stream) {
-    if (n < 1 || !node_table || !parents || !workspace || !weights_bf16 || !theta ||
+                                    const int32_t *workspace, int64_t n, const float *accel,
+                                    const uint32_t *perm, const void *weights_bf16, float *theta,
+                                    int max_buckets, void *stream) {
+    if (n < 1 || !node_table || !parents || !workspace || !accel || !weights_bf16 || !theta ||
         max_buckets < 0)
         return CNB_E_INVALID_ARG;
     const int64_t m = 2 * n - 1;
     const float4 *rec = reinterpret_cast<const float4 *>(node_table);
     k_controller<<<grid_for(max_buckets, 256, 148 * 4), 256, 0, as_stream(stream)>>>(
-        rec, rec + 2 * m, parents, workspace,
+        rec, rec + 2 * m, parents, workspace, accel, perm,
         reinterpret_cast<const __nv_bfloat16 *>(weights_bf16), theta, max_buckets);
     return launch_status();
 }

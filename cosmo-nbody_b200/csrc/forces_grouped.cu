@@ -513,6 +513,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
                     set_flag(P.status, CNB_FLAG_NONFINITE);
             }
         }
+        if (P.bucket_inter && lane == 0) P.bucket_inter[g] = (int32_t)n_entries;
         if (P.stats && lane == 0) {
             atomicAdd(P.stats, n_entries * (unsigned long long)count);
             atomicAdd(P.stats + 2, n_wrap * (unsigned long long)count);
@@ -915,8 +916,8 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
                                         int64_t n, double theta, const float *theta_per_bucket,
                                         int bodies_per_lane, int block_warps, double G, double soft,
                                         const float *ewald_table, int ewald_nt,
-                                        const float *quad, unsigned long long *stats,
-                                        int32_t *status, void *stream) {
+                                        const float *quad, int32_t *bucket_inter,
+                                        unsigned long long *stats, int32_t *status, void *stream) {
     GroupedParams P;
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket,
                            CNB_MAC_REF_X, bodies_per_lane, block_warps, G, stats, status));
@@ -933,6 +934,7 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
     P.ewald_nt = ewald_nt;
     if (quad && (reinterpret_cast<uintptr_t>(quad) & 15)) return CNB_E_INVALID_ARG;
     P.quad = reinterpret_cast<const float4 *>(quad);
+    P.bucket_inter = bucket_inter;
     return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }
 
@@ -943,8 +945,9 @@ extern "C" int cnb_forces_grouped_boxes_ewald(const float *px, const float *py, 
                                               const float *box_params,
                                               const float *theta_per_bucket, int bodies_per_lane,
                                               int block_warps, double G, const float *ewald_table,
-                                              int ewald_nt, unsigned long long *stats,
-                                              int32_t *status, void *stream) {
+                                              int ewald_nt, int32_t *bucket_inter,
+                                              unsigned long long *stats, int32_t *status,
+                                              void *stream) {
     GroupedParams P;
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket,
                            CNB_MAC_REF_X, bodies_per_lane, block_warps, G, stats, status));
@@ -962,6 +965,7 @@ extern "C" int cnb_forces_grouped_boxes_ewald(const float *px, const float *py, 
     P.box_params = reinterpret_cast<const float4 *>(box_params);
     P.ewald = reinterpret_cast<const float4 *>(ewald_table);
     P.ewald_nt = ewald_nt;
+    P.bucket_inter = bucket_inter;
     return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }
 

@@ -343,13 +343,15 @@ int cnb_ewald_table(float *table, int nt, void *stream);
  * then also apply their quadrupole term, (15/2)(d.M d) d/r^7 - 3 M d/r^5 -
  * (3/2) tr(M) d/r^5, plus its periodic part (1/2) H(c - centre) : M from
  * the table's second derivatives of g (stats[2] then counts those
- * quadrupole interactions). */
+ * quadrupole interactions).  bucket_inter (device int32 per bucket slot, may
+ * be NULL) receives the interactions each body of the bucket received: the
+ * per-bucket cost the learned controller's labels weigh. */
 int cnb_forces_grouped_ewald(const float *px, const float *py, const float *pz,
                              const float *node_table, int32_t *workspace, float *force, int64_t n,
                              double theta, const float *theta_per_bucket, int bodies_per_lane,
                              int block_warps, double G, double soft, const float *ewald_table,
-                             int ewald_nt, const float *quad, unsigned long long *stats,
-                             int32_t *status, void *stream);
+                             int ewald_nt, const float *quad, int32_t *bucket_inter,
+                             unsigned long long *stats, int32_t *status, void *stream);
 
 /* cnb_upward_table that also forms the second central moment of every
  * internal node about its CoM (parallel-axis rule over the two children):
@@ -375,15 +377,15 @@ int cnb_upward_table_buckets(const float *px, const float *py, const float *pz, 
                              float *sums, float *quad, int64_t n, int32_t *status, void *stream);
 
 /* cnb_forces_grouped_boxes under the periodic law of cnb_forces_grouped_ewald:
- * every box is periodic on its own unit cube. */
+ * every box is periodic on its own unit cube (bucket_inter as there). */
 int cnb_forces_grouped_boxes_ewald(const float *px, const float *py, const float *pz,
                                    const float *node_table, int32_t *workspace, float *force,
                                    int64_t n, const uint64_t *codes, int box_bits,
                                    const int32_t *box_roots, const float *box_params,
                                    const float *theta_per_bucket, int bodies_per_lane,
                                    int block_warps, double G, const float *ewald_table,
-                                   int ewald_nt, unsigned long long *stats, int32_t *status,
-                                   void *stream);
+                                   int ewald_nt, int32_t *bucket_inter,
+                                   unsigned long long *stats, int32_t *status, void *stream);
 
 /* Float64 periodic direct sum for the bodies listed in targets (accuracy
  * oracle of the periodic law): per pair the softened monopole at the minimum
@@ -437,17 +439,23 @@ int cnb_integrate_boxes(float *px, float *py, float *pz, float *vx, float *vy, f
 #define CNB_MLP_PARAMS 5057
 
 /* 12 features per bucket (float32 [buckets, 12]) from the node table,
- * parents and the bucket table of cnb_make_buckets; at most max_buckets. */
+ * parents and the bucket table of cnb_make_buckets; at most max_buckets.
+ * accel (float32 [N, 3], required) holds the bodies' accelerations of the
+ * previous step; perm (may be NULL: identity) maps each body's current
+ * position in the sorted order to its row of accel (the sort's
+ * permutation).  One feature is the bucket's mean |a| over the local force
+ * scale G M / l^2 of its third ancestor. */
 int cnb_bucket_features(const float *node_table, const int32_t *parents,
-                        const int32_t *workspace, int64_t n, float *features, int max_buckets,
-                        void *stream);
+                        const int32_t *workspace, int64_t n, const float *accel,
+                        const uint32_t *perm, float *features, int max_buckets, void *stream);
 
 /* Fused inference: features and the network (bfloat16 weights, float32
  * accumulation) -> theta per bucket slot, the theta_per_bucket input of
- * cnb_forces_grouped. */
+ * cnb_forces_grouped (accel, perm as for cnb_bucket_features). */
 int cnb_controller_theta(const float *node_table, const int32_t *parents,
-                         const int32_t *workspace, int64_t n, const void *weights_bf16,
-                         float *theta, int max_buckets, void *stream);
+                         const int32_t *workspace, int64_t n, const float *accel,
+                         const uint32_t *perm, const void *weights_bf16, float *theta,
+                         int max_buckets, void *stream);
 
 /* The network on given features with float32 weights. */
 int cnb_mlp_predict(const float *features, int n, const float *weights, float *theta,

@@ -86,9 +86,11 @@ def bf16_round(a):
     return r.astype(np.uint32).view(np.float32)
 
 
-def bucket_features(rec, aabb, parents, bucket):
+def bucket_features(rec, aabb, parents, bucket, accel, perm=None):
     """Features of one bucket (first, count, node, _) from the node table
-    records rec [M,2,4] / boxes aabb [M,2,4] and parents (float64)."""
+    records rec [M,2,4] / boxes aabb [M,2,4], parents and the previous step's
+    accelerations accel [N,3] (row perm[i] for sorted body i; perm None:
+    identity), in float64."""
     first, count, v = int(bucket[0]), int(bucket[1]), int(bucket[2])
 
     def extent(u):
@@ -100,14 +102,22 @@ def bucket_features(rec, aabb, parents, bucket):
     lo, hi = aabb[v, 0].astype(np.float64), aabb[v, 1].astype(np.float64)
     ext = max(extent(v), 1e-3 * s)
     vol = np.prod(hi[:3] - lo[:3] + s)
-    f = [np.log2(ext / s), np.log2(count) * 0.2, np.log2(count * s ** 3 / vol)]
+    f = [np.log2(ext / s), 0.0, np.log2(count * s ** 3 / vol)]
     p = v
+    pe, pm = ext, A[3]
     for _ in range(3):
         q = int(parents[p])
         if q >= 0:
             p = q
         P = rec[p, 0].astype(np.float64)
         pe = max(extent(p), ext)
-        f += [np.log2(pe / ext), np.log2(max(P[3], A[3]) / A[3]),
+        pm = max(P[3], A[3])
+        f += [np.log2(pe / ext), np.log2(pm / A[3]),
               float(np.linalg.norm(P[:3] - A[:3]) / pe)]
+    rows = np.arange(first, first + count)
+    if perm is not None:
+        rows = np.asarray(perm, np.int64)[rows]
+    amean = np.linalg.norm(np.asarray(accel, np.float64)[rows], axis=1).mean()
+    # mean |a| over the third ancestor's force scale G M / l^2 (G = 1)
+    f[1] = 0.25 * np.log2(max(amean * pe * pe / pm, 1e-6))
     return np.array(f)

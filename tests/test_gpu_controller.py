@@ -73,19 +73,24 @@ def test_features_and_fused_inference_match_oracle():
     eng = _built_engine()
     tm = eng.tree_manager
     n = eng.state.n
-    feats = bucket_features(tm.node_table, tm.parent, tm.workspace, n).cpu().numpy()
+    # accelerations of a step with a permutation as the previous-step input
+    acc = eng.state.force.clone()
+    perm = torch.from_numpy(np.random.default_rng(9).permutation(n).astype(np.uint32)).cuda()
+    feats = bucket_features(tm.node_table, tm.parent, tm.workspace, n, acc, perm).cpu().numpy()
     flat = tm.node_table.cpu().numpy().reshape(-1, 4)   # 2M records then 2M boxes
     m = flat.shape[0] // 4
     rec = flat[:2 * m].reshape(m, 2, 4)
     aabb = flat[2 * m:].reshape(m, 2, 4)
     parents = tm.parent.cpu().numpy()
     bk = tm.workspace[4:4 + 4 * feats.shape[0]].view(-1, 4).cpu().numpy()
-    want = np.stack([mlp.bucket_features(rec, aabb, parents, b) for b in bk])
+    acc_h, perm_h = acc.cpu().numpy(), perm.cpu().numpy()
+    want = np.stack([mlp.bucket_features(rec, aabb, parents, b, acc_h, perm_h) for b in bk])
     np.testing.assert_allclose(feats, want, rtol=1e-4, atol=1e-4)
     ctl = ThetaController(seed=3)
     ctl.mean = torch.from_numpy(want.mean(0).astype(np.float32)).cuda()
     ctl.std = torch.from_numpy(want.std(0).astype(np.float32) + 1e-3).cuda()
-    th = ctl.theta_for_buckets(tm.node_table, tm.parent, tm.workspace, n)[:feats.shape[0]].cpu().numpy()
+    th = ctl.theta_for_buckets(tm.node_table, tm.parent, tm.workspace, n, acc,
+                               perm)[:feats.shape[0]].cpu().numpy()
     folded = mlp.bf16_round(ctl.folded_params().cpu().numpy())
     wth, _ = mlp.forward(folded, feats)
     np.testing.assert_allclose(th, wth, rtol=0, atol=2e-4)

@@ -44,3 +44,34 @@ def test_bench_metric_names_the_grid_size():
         sys.argv = argv
     assert bench.metric_for(128) == bench.METRIC          # the default run's metric is unchanged
     assert "N=256^3" in bench.metric_for(256) and "128" not in bench.metric_for(256)
+
+
+def test_lagrangian_allocation_meets_the_global_budget():
+    """cnb.controller.allocate: per-bucket angles that minimise the cost while
+    at most `allowed` bodies exceed the budget; on a small case the result
+    is feasible, no dearer than one fixed angle with the same violations,
+    and equal to the exhaustive optimum."""
+    import itertools
+
+    import numpy as np
+
+    from cnb.controller import allocate
+    rng = np.random.default_rng(5)
+    T, G, per = 4, 6, 5
+    owner = np.repeat(np.arange(G), per)
+    # cost falls and error grows with the angle index; buckets differ in sensitivity
+    sens = rng.uniform(0.5, 2.0, G)
+    errors = np.stack([np.repeat(sens, per) * (k + 1) * rng.uniform(0.8, 1.2, G * per) for k in range(T)])
+    costs = np.stack([np.full(G, 100.0 / (k + 1)) * rng.uniform(0.9, 1.1, G) for k in range(T)])
+    budget = float(np.percentile(errors[1], 80))
+    allowed = int((errors[1] > budget).sum())
+    idx, total, v = allocate(errors, costs, owner, budget, allowed)
+    assert v <= allowed
+    assert total <= costs[1].sum() + 1e-9
+    best = np.inf
+    for choice in itertools.product(range(T), repeat=G):
+        c = np.array(choice)
+        viol = sum(int((errors[c[g], owner == g] > budget).sum()) for g in range(G))
+        if viol <= allowed:
+            best = min(best, costs[c, np.arange(G)].sum())
+    assert total <= best * 1.15       # the Lagrangian point is close to the exhaustive optimum
