@@ -101,7 +101,8 @@ SIGNATURES = {
     "cnb_colorize": (_int, [_p, _int, _int, _p, _p, _p, _p]),
     "cnb_ewald_table": (_int, [_p, _int, _p]),
     "cnb_forces_grouped_ewald": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _d, _d, _p,
-                                        _int, _p, _p, _p, _p, _p]),
+                                        _int, _p, _p, _p, _p, _p, _p]),
+    "cnb_order_buckets": (_int, [_p, _p, _p, _p]),
     "cnb_upward_table_quad": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_upward_table_buckets": (_int, [_p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _p, _i64, _p, _p]),
     "cnb_direct_sum_ewald_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),

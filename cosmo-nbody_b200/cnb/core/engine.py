@@ -72,6 +72,7 @@ class SimulationEngine:
         # the controller's acceleration input: None = the previous step's forces
         # (state.force); a tensor [N, 3] in the current sorted order overrides it
         self.controller_accel = None
+        self._bucket_order = None
         # True while state.force holds forces in the current sorted order (a
         # sort since the last force stage leaves it in the previous order)
         self._force_current = False
@@ -139,6 +140,14 @@ class SimulationEngine:
                     tm.node_table, tm.parent, tm.workspace, s.n, accel, perm,
                     out=self.theta_per_group, scale=self.controller_scale)
             tpg = self.theta_per_group
+            order = None
+            if self.ewald_table is not None and tpg is not None:
+                # per-bucket angles: the most expensive buckets are handed out first
+                if self._bucket_order is None or self._bucket_order.numel() < tpg.numel():
+                    self._bucket_order = torch.empty(tpg.numel(), dtype=torch.int32, device=s.device)
+                order = self._bucket_order
+                _lib.call("cnb_order_buckets", tpg.data_ptr(), tm.workspace.data_ptr(),
+                          order.data_ptr(), st)
             if self.ewald_table is not None:
                 _lib.call("cnb_forces_grouped_ewald", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
                           tm.node_table.data_ptr(), tm.workspace.data_ptr(), s.force.data_ptr(), s.n,
@@ -146,6 +155,7 @@ class SimulationEngine:
                           self.bodies_per_lane, self.block_warps, float(cfg.G), float(cfg.SOFTENING),
                           self.ewald_table.data_ptr(), EWALD_NT,
                           tm.quad.data_ptr() if tm.quad is not None else None,
+                          order.data_ptr() if order is not None else None,
                           self.bucket_inter.data_ptr() if self.bucket_inter is not None else None,
                           self.stats.data_ptr(), status, st)
                 return

@@ -211,6 +211,20 @@ def batched(args):
                           speedup=seq_ms / batched_ms)), flush=True)
 
 
+def _time_forces(eng, reps=3):
+    """Best of `reps` CUDA-event timings of the engine's force stage."""
+    eng.compute_forces()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        eng.compute_forces()
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
 def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
     """The cheapest per-bucket allocation of theta on the engine's current
     tree at the same global error percentile as plain theta = 0.5: every
@@ -247,11 +261,50 @@ def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
     allowed = int((errs[k05] > budget).sum())
     idx, total, v = allocate(errs, costs, owner, budget, allowed)
     chosen = np.asarray(thetas)[idx]
+    # the allocation itself run through the kernel: its force time
+    alloc = torch.from_numpy(chosen.astype(np.float32)).to(s.pos[0].device)
+    eng.theta_per_group = alloc
+    eng.controller = None
+    ms = _time_forces(eng)
+    eng.theta_per_group, eng.controller = saved
     return dict(bound=float(costs[k05].sum() / total), budget_rel=budget, allowed=allowed,
+                forces_ms_allocation=ms, theta_allocation=alloc,
                 violations=v, buckets=nb,
                 theta_hist={f"{t:.1f}": int((chosen == t).sum()) for t in thetas},
                 interactions_per_body_plain=float(costs[k05].sum() / s.n),
                 interactions_per_body_bound=float(total / s.n))
+
+
+def _reference_tree_forces(n_grid, pos, vel, bpl):
+    """Periodic-law forces of every body with quadrupoles at theta = 0.2 (in
+    the same sorted order as an engine built on the same bodies)."""
+    n = n_grid ** 3
+    qeng = SimulationEngine(_cfg(n_grid, MAC="ewald", QUADRUPOLE=True, THETA=0.2,
+                                 BODIES_PER_LANE=bpl, BLOCK_WARPS=4),
+                            SimulationState(n, pos, vel), camera=False)
+    qeng.forces_only()
+    qeng.check()
+    return qeng.state.force.double(), qeng
+
+
+def _state_labels(n_grid, seed, evolve, bpl):
+    """(features, labels, info) of every bucket of an evolved n_grid^3 state:
+    the Lagrangian allocation at plain theta = 0.5's p99 against the
+    reference-accuracy tree."""
+    from .controller import bucket_features
+    pos, vel, _ = _evolve(n_grid, seed, evolve)
+    n = n_grid ** 3
+    eng = SimulationEngine(_cfg(n_grid, MAC="ewald", BODIES_PER_LANE=bpl, BLOCK_WARPS=4),
+                           SimulationState(n, pos, vel), camera=False)
+    eng.forces_only()
+    acc = eng.state.force.clone()
+    ref, _ = _reference_tree_forces(n_grid, pos, vel, bpl)
+    b = lagrangian_bound(eng, ref)
+    alloc = b.pop("theta_allocation")
+    tm = eng.tree_manager
+    feats = bucket_features(tm.node_table, tm.parent, tm.workspace, n, acc)
+    nb = alloc.numel()
+    return feats[:nb], alloc, dict(seed=seed, buckets=nb, bound=b["bound"])
 
 
 def controller(args):
@@ -261,11 +314,23 @@ def controller(args):
     128^3 state, and the trained network against plain theta = 0.5 there at
     matched p99 (relative error; against a reference-accuracy tree on every
     body and against the float64 Ewald direct sum on a sample)."""
-    from .controller import ThetaController, make_labels
+    from .controller import ThetaController, bucket_features, make_labels
     t0 = time.time()
-    train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac="ewald", bodies_per_lane=args.bpl)
-    X, y, info = make_labels(train, per_box=args.per_box, error="relative")
-    del train
+    Xs, ys, info = [], [], {}
+    if args.labels in ("boxes", "both"):
+        train = BatchedBoxes(draw_boxes(args.boxes, seed=3), mac="ewald", bodies_per_lane=args.bpl)
+        X, y, info = make_labels(train, per_box=args.per_box, error="relative")
+        Xs.append(X)
+        ys.append(y)
+        del train
+    if args.labels in ("state", "both"):
+        # a second evolved state of the same recipe (seed 5): the allocation of
+        # every bucket against a reference-accuracy tree, as labels
+        tx, ty, tinfo = _state_labels(args.n_grid, 5, args.evolve, args.bpl)
+        Xs.append(tx)
+        ys.append(ty)
+        info = dict(info, state_labels=tinfo)
+    X, y = torch.cat(Xs), torch.cat(ys)
     ctl = ThetaController(seed=0)
     curve = ctl.train(X, y, steps=args.train_steps, lr=3e-3, over_weight=args.over_weight)
     if args.save:
@@ -278,17 +343,23 @@ def controller(args):
     eng.forces_only()
     plain_acc = eng.state.force.clone()
     # reference-accuracy forces on every body: quadrupoles at theta = 0.2 (same sort)
-    qeng = SimulationEngine(_cfg(args.n_grid, MAC="ewald", QUADRUPOLE=True, THETA=0.2,
-                                 BODIES_PER_LANE=args.bpl, BLOCK_WARPS=4),
-                            SimulationState(n, pos, vel), camera=False)
-    qeng.forces_only()
-    ref_tree = qeng.state.force.double()
+    ref_tree, qeng = _reference_tree_forces(args.n_grid, pos, vel, args.bpl)
     targets = np.sort(np.random.default_rng(0).choice(n, args.sample, replace=False)).astype(np.int64)
     ref_direct = _direct(eng.state, targets, eng.config.SOFTENING, periodic=True)
     tree_err = _errors(qeng.state.force, ref_direct, targets)
     del qeng
     bound = lagrangian_bound(eng, ref_tree)
-    T = torch.from_numpy(targets).cuda()
+    alloc = bound.pop("theta_allocation")
+    # cost curve of uniform theta on this state
+    curve_rows = []
+    for th in (0.4, 0.5, 0.6, 0.7, 0.8):
+        eng.theta_per_group = None
+        eng.config.THETA = th
+        eng.stats.zero_()
+        eng.compute_forces()
+        inter = float(eng.stats[0].item()) / n
+        curve_rows.append(dict(theta=th, interactions=inter, forces_ms=_time_forces(eng)))
+    eng.config.THETA = 0.5
 
     def run(scale=None):
         eng.controller = ctl if scale is not None else None
@@ -316,13 +387,31 @@ def controller(args):
         r = run(mid)
         lo, hi = (mid, hi) if r[key] <= plain[key] else (lo, mid)
     learned = run(lo)
+    # the network's angles alone through the force kernel (inference outside the timing)
+    th_l = eng.theta_per_group.clone()
     eng.controller = None
+    eng.theta_per_group = th_l
+    learned["forces_ms_without_inference"] = _time_forces(eng)
+    eng.controller, eng.controller_scale = ctl, lo
+    tm = eng.tree_manager
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    ctl.theta_for_buckets(tm.node_table, tm.parent, tm.workspace, n, plain_acc, None, out=th_l, scale=lo)
+    e1.record()
+    torch.cuda.synchronize()
+    learned["inference_ms"] = e0.elapsed_time(e1)
+    nb = int(tm.workspace[0].item())
+    learned["theta_hist"] = np.histogram(th_l[:nb].cpu().numpy(), bins=8, range=(0.2, 1.0))[0].tolist()
+    eng.controller = None
+    eng.theta_per_group = None
     eng.controller_accel = None
     eng.check()
     gain = plain["interactions"] / learned["interactions"]
     print(json.dumps(dict(study="controller", law="ewald", n_grid=args.n_grid, evolve_steps=args.evolve,
+                          training=dict(labels=args.labels, samples=int(y.numel()),
+                                        over_weight=args.over_weight),
                           a=a, labels=info, train_loss=[curve[0], curve[-1]], train_seconds=t_train,
-                          reference_tree_vs_direct=tree_err, bound=bound,
+                          reference_tree_vs_direct=tree_err, bound=bound, uniform_theta=curve_rows,
                           plain_theta05=plain, learned=learned, learned_scale=lo,
                           gain_interactions=gain, gain_forces_ms=plain["ms"] / learned["ms"],
                           fraction_of_bound=gain / bound["bound"],
@@ -385,6 +474,9 @@ def main():
     ap.add_argument("--over-weight", type=float, default=4.0,
                     help="controller training: weight of over-estimated theta in the loss")
     ap.add_argument("--save", default=None, help="controller study: write the trained weights here")
+    ap.add_argument("--labels", default="boxes", choices=["boxes", "state", "both"],
+                    help="controller study: train on the batched boxes' labels, on the allocation "
+                         "of a second evolved state (seed 5), or both")
     ap.add_argument("--bpl", type=int, default=1, choices=[1, 2])
     args = ap.parse_args()
     if args.study == "precision":

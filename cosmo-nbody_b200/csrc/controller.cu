@@ -41,9 +41,23 @@ __device__ __forceinline__ float node_extent(const float4 *aabb, int v) {
     return fmaxf(hi.x - lo.x, fmaxf(hi.y - lo.y, hi.z - lo.z));
 }
 
+// Mean |a| of a bucket's bodies (previous step; row perm[i] of accel for
+// sorted body i), by one thread.
+__device__ float bucket_mean_accel(const float *__restrict__ accel, const uint32_t *__restrict__ perm,
+                                   int4 bk) {
+    float amean = 0.f;
+    for (int k = 0; k < bk.y; ++k) {
+        const int64_t i = (int64_t)bk.x + k;
+        const int64_t r = perm ? (int64_t)perm[i] : i;
+        const float ax = accel[3 * r], ay = accel[3 * r + 1], az = accel[3 * r + 2];
+        amean += sqrtf(ax * ax + ay * ay + az * az);
+    }
+    return amean / (float)bk.y;
+}
+
 __device__ void bucket_features(const float4 *__restrict__ rec, const float4 *__restrict__ aabb,
-                                const int32_t *__restrict__ parents, const float *__restrict__ accel,
-                                const uint32_t *__restrict__ perm, int4 bk, float f[kIn]) {
+                                const int32_t *__restrict__ parents, float amean, int4 bk,
+                                float f[kIn]) {
     const int v = bk.z;
     const float4 A = rec[2 * v];
     const float m_body = A.w / (float)bk.y;
@@ -66,14 +80,6 @@ __device__ void bucket_features(const float4 *__restrict__ rec, const float4 *__
         f[4 + 3 * k] = __log2f(pm / A.w);
         f[5 + 3 * k] = sqrtf(dx * dx + dy * dy + dz * dz) / pe;
     }
-    float amean = 0.f;
-    for (int k = 0; k < bk.y; ++k) {
-        const int64_t i = (int64_t)bk.x + k;
-        const int64_t r = perm ? (int64_t)perm[i] : i;
-        const float ax = accel[3 * r], ay = accel[3 * r + 1], az = accel[3 * r + 2];
-        amean += sqrtf(ax * ax + ay * ay + az * az);
-    }
-    amean /= (float)bk.y;
     // G = 1 in the box's units: the scale is the third ancestor's M / l^2
     f[1] = 0.25f * __log2f(fmaxf(amean * pe * pe / pm, 1e-6f));
 }
@@ -89,7 +95,8 @@ __global__ void __launch_bounds__(256) k_features(const float4 *__restrict__ rec
     const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
         float f[kIn];
-        bucket_features(rec, aabb, parents, accel, perm, buckets[g], f);
+        const int4 bk = buckets[g];
+        bucket_features(rec, aabb, parents, bucket_mean_accel(accel, perm, bk), bk, f);
 #pragma unroll
         for (int k = 0; k < kIn; ++k) out[(int64_t)g * kIn + k] = f[k];
     }
@@ -121,25 +128,66 @@ __device__ __forceinline__ float theta_of(float z) {
     return kThetaLo + (kThetaHi - kThetaLo) * sigmoidf_(z);
 }
 
-// Fused inference: features of each bucket and the network on bfloat16
-// weights (converted once per block into float32 shared memory).
-__global__ void __launch_bounds__(256) k_controller(const float4 *__restrict__ rec,
-                                                    const float4 *__restrict__ aabb,
-                                                    const int32_t *__restrict__ parents,
-                                                    const int32_t *__restrict__ ws,
-                                                    const float *__restrict__ accel,
-                                                    const uint32_t *__restrict__ perm,
-                                                    const __nv_bfloat16 *__restrict__ wbf,
-                                                    float *__restrict__ theta, int max_buckets) {
+// Fused inference, one warp per bucket: the lanes read the bucket's
+// accelerations (coalesced) and form its features, then the network with
+// the bfloat16 weights converted once per block into float32 shared memory
+// (W2 transposed so that lane k reads row k of every column): lane j owns
+// hidden units j and j + 32 of both layers, the output is a warp sum.
+constexpr int kCtlWarps = 8;
+__global__ void __launch_bounds__(kCtlWarps * 32) k_controller(const float4 *__restrict__ rec,
+                                                             const float4 *__restrict__ aabb,
+                                                             const int32_t *__restrict__ parents,
+                                                             const int32_t *__restrict__ ws,
+                                                             const float *__restrict__ accel,
+                                                             const uint32_t *__restrict__ perm,
+                                                             const __nv_bfloat16 *__restrict__ wbf,
+                                                             float *__restrict__ theta, int max_buckets) {
     __shared__ float w[kParams];
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) w[i] = __bfloat162float(wbf[i]);
+    __shared__ float hbuf[kCtlWarps][kH];
+    for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
+        int dst = i;
+        if (i >= kOffW2 && i < kOffB2) {
+            const int k = (i - kOffW2) / kH, j = (i - kOffW2) % kH;  // W2[k][j]
+            dst = kOffW2 + j * kH + k;
+        }
+        w[dst] = __bfloat162float(wbf[i]);
+    }
     __syncthreads();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const int nb = min(ws[0], max_buckets);
     const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
+    for (int g = blockIdx.x * kCtlWarps + wib; g < nb; g += gridDim.x * kCtlWarps) {
+        const int4 bk = buckets[g];
+        float asum = 0.f;
+        for (int k = lane; k < bk.y; k += 32) {
+            const int64_t i = (int64_t)bk.x + k;
+            const int64_t r = perm ? (int64_t)perm[i] : i;
+            const float ax = accel[3 * r], ay = accel[3 * r + 1], az = accel[3 * r + 2];
+            asum += sqrtf(ax * ax + ay * ay + az * az);
+        }
+        for (int o = 16; o > 0; o >>= 1) asum += __shfl_xor_sync(0xffffffffu, asum, o);
         float f[kIn];
-        bucket_features(rec, aabb, parents, accel, perm, buckets[g], f);
-        theta[g] = theta_of(mlp_forward(w, f));
+        bucket_features(rec, aabb, parents, asum / (float)bk.y, bk, f);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int j = lane + 32 * u;
+            float a = w[kOffB1 + j];
+#pragma unroll
+            for (int i = 0; i < kIn; ++i) a = fmaf(w[kOffW1 + j * kIn + i], f[i], a);
+            hbuf[wib][j] = siluf_(a);
+        }
+        __syncwarp();
+        float a0 = w[kOffB2 + lane], a1 = w[kOffB2 + lane + 32];
+#pragma unroll 8
+        for (int j = 0; j < kH; ++j) {
+            const float h = hbuf[wib][j];
+            a0 = fmaf(w[kOffW2 + j * kH + lane], h, a0);
+            a1 = fmaf(w[kOffW2 + j * kH + lane + 32], h, a1);
+        }
+        float z = fmaf(w[kOffW3 + lane], siluf_(a0), w[kOffW3 + lane + 32] * siluf_(a1));
+        for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
+        if (lane == 0) theta[g] = theta_of(z + w[kOffB3]);
+        __syncwarp();
     }
 }
 
@@ -326,7 +374,7 @@ extern "C" int cnb_controller_theta(const float *node_table, const int32_t *pare
         return CNB_E_INVALID_ARG;
     const int64_t m = 2 * n - 1;
     const float4 *rec = reinterpret_cast<const float4 *>(node_table);
-    k_controller<<<grid_for(max_buckets, 256, 148 * 4), 256, 0, as_stream(stream)>>>(
+    k_controller<<<grid_for(max_buckets, kCtlWarps, 148 * 8), kCtlWarps * 32, 0, as_stream(stream)>>>(
         rec, rec + 2 * m, parents, workspace, accel, perm,
         reinterpret_cast<const __nv_bfloat16 *>(weights_bf16), theta, max_buckets);
     return launch_status();

@@ -280,6 +280,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
         if (lane == 0) g = atomicAdd(P.ws + 1, 1);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= n_buckets) break;
+        if (P.bucket_order) g = P.bucket_order[g];
         const int4 bk = P.buckets[g];
         const int count = bk.y;
         float x[BPL], y[BPL], z[BPL];

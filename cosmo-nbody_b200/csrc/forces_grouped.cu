@@ -215,6 +215,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
         if (lane == 0) g = atomicAdd(P.ws + 1, 1);
         g = __shfl_sync(0xffffffffu, g, 0);
         if (g >= n_buckets) break;
+        if (P.bucket_order) g = P.bucket_order[g];
         const int4 bk = P.buckets[g];
         const int count = bk.y;
         float x[BPL], y[BPL], z[BPL];
@@ -710,9 +711,46 @@ __global__ void __launch_bounds__(256) k_pack_nodes(const float *__restrict__ n_
     }
 }
 
+// Heaviest buckets first: a counting sort of the bucket slots by theta in
+// 32 bins over [0.2, 1.0] (smallest theta = most interactions first), so the
+// persistent traversal does not end on a few expensive buckets.  One block;
+// the order inside a bin is whatever the atomics give (each bucket's result
+// does not depend on when it runs).
+constexpr int kOrderBins = 32;
+__global__ void __launch_bounds__(1024) k_order_buckets(const float *__restrict__ theta,
+                                                        const int32_t *__restrict__ ws,
+                                                        int32_t *__restrict__ order) {
+    __shared__ int32_t cnt[kOrderBins], start[kOrderBins];
+    const int nb = ws[0];
+    if (threadIdx.x < kOrderBins) cnt[threadIdx.x] = 0;
+    __syncthreads();
+    auto bin_of = [](float t) {
+        const int b = (int)((t - 0.2f) * (kOrderBins / 0.8f));
+        return b < 0 ? 0 : (b >= kOrderBins ? kOrderBins - 1 : b);
+    };
+    for (int g = threadIdx.x; g < nb; g += blockDim.x) atomicAdd(&cnt[bin_of(theta[g])], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = 0; b < kOrderBins; ++b) {
+            start[b] = run;
+            run += cnt[b];
+        }
+    }
+    __syncthreads();
+    for (int g = threadIdx.x; g < nb; g += blockDim.x) order[atomicAdd(&start[bin_of(theta[g])], 1)] = g;
+}
+
 }  // namespace cnb
 
 using namespace cnb;
+
+extern "C" int cnb_order_buckets(const float *theta_per_bucket, const int32_t *workspace,
+                                 int32_t *order, void *stream) {
+    if (!theta_per_bucket || !workspace || !order) return CNB_E_INVALID_ARG;
+    k_order_buckets<<<1, 1024, 0, as_stream(stream)>>>(theta_per_bucket, workspace, order);
+    return launch_status();
+}
 
 extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const float *n_min,
                               const float *n_max, const int32_t *children, float *node_table,
@@ -916,8 +954,9 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
                                         int64_t n, double theta, const float *theta_per_bucket,
                                         int bodies_per_lane, int block_warps, double G, double soft,
                                         const float *ewald_table, int ewald_nt,
-                                        const float *quad, int32_t *bucket_inter,
-                                        unsigned long long *stats, int32_t *status, void *stream) {
+                                        const float *quad, const int32_t *bucket_order,
+                                        int32_t *bucket_inter, unsigned long long *stats,
+                                        int32_t *status, void *stream) {
     GroupedParams P;
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, theta_per_bucket,
                            CNB_MAC_REF_X, bodies_per_lane, block_warps, G, stats, status));
@@ -934,6 +973,7 @@ extern "C" int cnb_forces_grouped_ewald(const float *px, const float *py, const 
     P.ewald_nt = ewald_nt;
     if (quad && (reinterpret_cast<uintptr_t>(quad) & 15)) return CNB_E_INVALID_ARG;
     P.quad = reinterpret_cast<const float4 *>(quad);
+    P.bucket_order = bucket_order;
     P.bucket_inter = bucket_inter;
     return launch_grouped(P, bodies_per_lane, block_warps, as_stream(stream));
 }

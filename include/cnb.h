@@ -345,13 +345,24 @@ int cnb_ewald_table(float *table, int nt, void *stream);
  * the table's second derivatives of g (stats[2] then counts those
  * quadrupole interactions).  bucket_inter (device int32 per bucket slot, may
  * be NULL) receives the interactions each body of the bucket received: the
- * per-bucket cost the learned controller's labels weigh. */
+ * per-bucket cost the learned controller's labels weigh.  bucket_order (may
+ * be NULL: slot order) is the order buckets are handed out in
+ * (cnb_order_buckets). */
 int cnb_forces_grouped_ewald(const float *px, const float *py, const float *pz,
                              const float *node_table, int32_t *workspace, float *force, int64_t n,
                              double theta, const float *theta_per_bucket, int bodies_per_lane,
                              int block_warps, double G, double soft, const float *ewald_table,
-                             int ewald_nt, const float *quad, int32_t *bucket_inter,
-                             unsigned long long *stats, int32_t *status, void *stream);
+                             int ewald_nt, const float *quad, const int32_t *bucket_order,
+                             int32_t *bucket_inter, unsigned long long *stats, int32_t *status,
+                             void *stream);
+
+/* No counterpart in the reference.  The order in which the grouped
+ * traversal should take the buckets of a per-bucket theta (the bucket_order
+ * input of cnb_forces_grouped_ewald): smallest theta, the most work, first,
+ * in 32 bins over [0.2, 1.0], so that the persistent launch does not end on
+ * a few expensive buckets.  order: device int32 per bucket slot. */
+int cnb_order_buckets(const float *theta_per_bucket, const int32_t *workspace, int32_t *order,
+                      void *stream);
 
 /* cnb_upward_table that also forms the second central moment of every
  * internal node about its CoM (parallel-axis rule over the two children):

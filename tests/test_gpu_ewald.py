@@ -118,7 +118,7 @@ class Tree:
         _lib.call("cnb_forces_grouped_ewald", *(p.data_ptr() for p in self.P),
                   self.tm.node_table.data_ptr(), self.tm.workspace.data_ptr(), f.data_ptr(), self.n,
                   theta, None, self.bpl, 4, 1.0, soft, self.table.data_ptr(), 64,
-                  self.tm.quad.data_ptr() if self.tm.quad is not None else None, None, stats.data_ptr(),
+                  self.tm.quad.data_ptr() if self.tm.quad is not None else None, None, None, stats.data_ptr(),
                   status.data_ptr(), _stream())
         torch.cuda.synchronize()
         assert int(status.item()) == 0
