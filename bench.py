@@ -92,6 +92,10 @@ def parse():
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch every kernel from Python instead of replaying a CUDA graph")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
+    ap.add_argument("--no-learned", dest="learned", action="store_false",
+                    help="skip the learned-theta against plain-theta comparison")
+    ap.add_argument("--learned-sample", type=int, default=4096,
+                    help="float64 periodic direct-sum sample of the learned-theta comparison")
     ap.add_argument("--profile", action="store_true",
                     help="timed loop only (no e2e, accuracy, CPU baseline or clock sampling)")
     return ap.parse_args()
@@ -478,6 +482,8 @@ def run_ours(args):
             # the reference's test decided once per bucket: finer node sets than the
             # reference's (not its forces), reported beside the headline
             line["variants"] = [variant(eng, args, "ref_x_bucket", flush)]
+        if args.learned and args.n_grid == 128 and args.force_mode == "grouped":
+            line["learned_vs_plain"] = learned_vs_plain(args, flush)
         if rank == 0:
             line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
@@ -523,6 +529,111 @@ def variant(eng, args, mac_name, flush):
     return {"mac": mac_name, "value": eng.state.n / (ms * 1e-3), "unit": "particle-steps/s",
             "ms_per_step": ms, "steps": 2 * reps, "forces_ms_eager": stages.get("forces"),
             "interactions_per_body": inter, "accuracy": acc}
+
+
+LEARNED_WEIGHTS = os.path.join(ROOT, "cosmo-nbody_b200", "cnb", "data", "theta_ewald.npz")
+
+
+def _timed_replays(eng, flush, reps=5):
+    """ms per step of `reps` replays of the engine's two-step graph, L2 flushed between."""
+    import torch
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(reps)]
+    for k in range(reps):
+        flush.zero_()
+        starts[k].record()
+        eng.replay()
+        ends[k].record()
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in zip(starts, ends)) / (2 * reps)
+
+
+def learned_vs_plain(args, flush):
+    """The headline metric's second half: on the evolved 128^3 state (seed 4,
+    100 steps of the plain recipe), plain theta = 0.5 against the learned
+    per-bucket theta under the periodic (Ewald) law, at matched p99 relative
+    force error against the float64 Ewald direct sum on a seeded sample.
+    The learned angles (committed weights) are scaled by one factor, bisected
+    so that their p99 does not exceed plain's; each arm is then timed as full
+    steps (CUDA-graph replays of two steps, L2 flushed).  Also reported: the
+    p99 of both arms on every body against a reference-accuracy tree
+    (quadrupoles, theta = 0.2), and the bound of any per-bucket policy on this
+    state (Lagrangian allocation at plain's p99 on every body)."""
+    import torch
+    from cnb.controller import ThetaController
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.studies import _cfg, _direct, _errors, _evolve, _reference_tree_forces, lagrangian_bound
+    if not os.path.exists(LEARNED_WEIGHTS):
+        return {"unavailable": "no trained weights (python -m cnb.studies controller --save ...)"}
+    n_grid, steps = 128, 100
+    n = n_grid ** 3
+    pos, vel, a = _evolve(n_grid, 4, steps)
+    cfg = _cfg(n_grid, MAC="ewald", BODIES_PER_LANE=2, BLOCK_WARPS=4, A_START=a,
+               A_END=a + 1000 * 0.002, RES=args.width, RES_W=args.width, RES_H=args.height)
+    eng = SimulationEngine(cfg, SimulationState(n, pos, vel))
+    eng.forces_only()
+    plain_acc = eng.state.force.clone()
+    ref_tree, qeng = _reference_tree_forces(n_grid, pos, vel, 2)
+    targets = np.sort(np.random.default_rng(0).choice(n, args.learned_sample, replace=False)).astype(np.int64)
+    t0 = time.time()
+    ref = _direct(eng.state, targets, cfg.SOFTENING, periodic=True)
+    direct_s = time.time() - t0
+    ref_self = _errors(qeng.state.force, ref, targets)
+    del qeng
+    ctl = ThetaController().load(LEARNED_WEIGHTS)
+
+    def evaluate(scale):
+        eng.controller = ctl if scale is not None else None
+        eng.controller_scale = scale or 1.0
+        eng.controller_accel = plain_acc
+        if scale is None:
+            eng.theta_per_group = None
+        eng.stats.zero_()
+        eng.compute_forces()
+        torch.cuda.synchronize()
+        e_all = (eng.state.force.double() - ref_tree).norm(dim=1) / ref_tree.norm(dim=1)
+        return dict(_errors(eng.state.force, ref, targets),
+                    p99_rel_every_body_vs_tree=float(torch.quantile(e_all.float(), 0.99).item()),
+                    interactions_per_body=float(eng.stats[0].item()) / n)
+
+    plain = evaluate(None)
+    lo, hi = 0.2, 3.0
+    for _ in range(14):
+        mid = 0.5 * (lo + hi)
+        lo, hi = (mid, hi) if evaluate(mid)["p99_rel"] <= plain["p99_rel"] else (lo, mid)
+    learned = evaluate(lo)
+    eng.controller_accel = None
+    bound = lagrangian_bound(eng, ref_tree)
+    bound.pop("theta_allocation")
+    out = {}
+    for name, scale, errs in (("plain", None, plain), ("learned", lo, learned)):
+        eng.controller = ctl if scale is not None else None
+        eng.controller_scale = scale or 1.0
+        eng.theta_per_group = None
+        eng.stats.zero_()
+        eng.enable_stage_timing(True)
+        for _ in range(2):
+            eng.step()
+        stages = {k: v / 2 for k, v in eng.stage_times().items()}
+        eng.enable_stage_timing(False)
+        eng.capture(splat=True)
+        ms = _timed_replays(eng, flush)
+        eng._graph = None
+        out[name] = dict(value=n / (ms * 1e-3), unit="particle-steps/s", ms_per_step=ms,
+                         forces_ms_eager=stages.get("forces"), theta="0.5" if scale is None else
+                         f"learned, scaled x{scale:.4f}", **errs)
+    eng.controller = None
+    eng.check()
+    return {"workload": f"Zel'dovich {n_grid}^3 seed 4 after {steps} steps (a = {a:.3f}), "
+                        "periodic (Ewald) law, monopoles, full step + splat",
+            "error": f"|a - a_ref| / |a_ref| against the float64 Ewald direct sum on {targets.size} "
+                     f"seeded bodies ({direct_s:.1f} s); reference tree on the same sample: "
+                     f"p99 {ref_self['p99_rel']:.3g}",
+            "plain": out["plain"], "learned": out["learned"],
+            "speedup": out["learned"]["value"] / out["plain"]["value"],
+            "interaction_ratio": plain["interactions_per_body"] / learned["interactions_per_body"],
+            "bound": bound, "weights": os.path.relpath(LEARNED_WEIGHTS, ROOT)}
 
 
 def accuracy(eng, args):
