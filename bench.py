@@ -66,7 +66,7 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
     ap.add_argument("--n-grid", type=int, default=N_GRID)
     ap.add_argument("--theta", type=float, default=0.5)
     ap.add_argument("--force-mode", default="grouped", choices=["grouped", "reference"])
@@ -325,6 +325,133 @@ def run_reference(args):
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+    return 0
+
+
+REF_STAGED = os.path.join(ROOT, "oracle", "_ref")
+
+
+def _spread21(v):
+    """21-bit Morton spread of int64 torch tensors (two zero bits between bits)."""
+    v = (v | (v << 32)) & 0x1F00000000FFFF
+    v = (v | (v << 16)) & 0x1F0000FF0000FF
+    v = (v | (v << 8)) & 0x100F00F00F00F00F
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3
+    v = (v | (v << 2)) & 0x1249249249249249
+    return v
+
+
+def run_reference_gpu(args):
+    """The reference's own Numba kernels on this GPU: src/kernels/*.py of
+    Cosmo-NBody, unmodified (staged into oracle/_ref by
+    oracle/stage_ref_gpu.sh), launched as its engine launches them
+    (src/core/engine.py:55-123, src/core/octree.py:45-83,
+    src/core/camera.py:29-48) with torch tensors as the device arrays in place
+    of CuPy: stable argsort and gathers by torch (cp.argsort and fancy
+    indexing in src/core/state.py:20-40), reset / build_tree /
+    compute_multipoles / normalize_com / find_root, the top-tree cache, the
+    force traversal in 5 000-body launches (engine.py:91-111), integrate, and
+    render_density on the reference's square 1024^2 grid.  One substitution:
+    the keys are the 63-bit Morton keys (torch bit interleave of the 21-bit
+    coordinates) in place of compute_codes' 30-bit keys of the low 10 bits of
+    each coordinate, with which the traversal visits O(N) nodes per body.
+    Numba 0.65 compiles for compute capability <= 9.0; its sm_90 PTX is
+    JIT-compiled by the driver for the B200."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    base = {"impl": "reference-gpu", "metric": metric_for(args.n_grid)}
+    if not os.path.isdir(os.path.join(REF_STAGED, "src", "kernels")):
+        print(json.dumps(dict(base, unavailable="reference kernels not staged (oracle/stage_ref_gpu.sh)")))
+        return 0
+    import types
+    import torch
+    from numba import cuda
+    from cnb.utils.cosmology import zeldovich_arrays
+    from cnb.utils.visualizer import get_mvp_matrix
+    sys.modules.setdefault("cupy", types.ModuleType("cupy"))   # imported, not used, by render_kernels
+    sys.path.insert(0, REF_STAGED)
+    from src.kernels.physics_kernels import compute_forces, integrate
+    from src.kernels.render_kernels import render_density
+    from src.kernels.tree_kernels import (build_top_tree_cache, build_tree, compute_multipoles,
+                                          find_root, normalize_com, reset_tree_buffers)
+    torch.cuda.set_device(0)
+    cfg = make_config(args, 1)
+    n = cfg.N_BODIES
+    m = 2 * n - 1
+    tpb, batch, cache, res = 256, 5000, 256, 1024
+    bpg, bpg_nodes = (n + tpb - 1) // tpb, (m + tpb - 1) // tpb
+    pos_h, vel_h = zeldovich_arrays(cfg.N_GRID, 1)
+    dev = torch.device("cuda", 0)
+    pos = [torch.from_numpy(p).to(dev) for p in pos_h]
+    vel = [torch.from_numpy(v).to(dev) for v in vel_h]
+    mass = torch.full((n,), 1.0 / n, dtype=torch.float32, device=dev)
+    child = torch.full((m, 2), -1, dtype=torch.int32, device=dev)
+    parent = torch.full((m,), -1, dtype=torch.int32, device=dev)
+    root = torch.zeros(1, dtype=torch.int32, device=dev)
+    n_mass = torch.zeros(m, dtype=torch.float32, device=dev)
+    n_com = torch.zeros((m, 3), dtype=torch.float32, device=dev)
+    n_min = torch.zeros((m, 3), dtype=torch.float32, device=dev)
+    n_max = torch.zeros((m, 3), dtype=torch.float32, device=dev)
+    counters = torch.zeros(m, dtype=torch.int32, device=dev)
+    force = torch.zeros((n, 3), dtype=torch.float32, device=dev)
+    top_nodes = torch.full((cache,), -1, dtype=torch.int32, device=dev)
+    node_to_cache = torch.full((m,), -1, dtype=torch.int32, device=dev)
+    grid = torch.zeros((res, res), dtype=torch.float32, device=dev)
+    A = cuda.as_cuda_array
+    st = {"a": cfg.A_START}
+
+    def step(i):
+        a = st["a"]
+        H = cfg.H0 * (cfg.OMEGA_M * a ** -3 + cfg.OMEGA_L) ** 0.5
+        dt = 0.002 / (a * H) * 0.8
+        ix = [torch.clamp((p.double() * 2097152.0).to(torch.int64), 0, 2097151) for p in pos]
+        keys = _spread21(ix[0]) | (_spread21(ix[1]) << 1) | (_spread21(ix[2]) << 2)
+        order = torch.argsort(keys, stable=True)
+        for lst in (pos, vel):
+            for k in range(3):
+                lst[k] = lst[k][order]
+        codes = keys[order].view(torch.uint64)
+        reset_tree_buffers[bpg_nodes, tpb](A(child), A(parent), A(counters), A(root))
+        build_tree[bpg, tpb](A(codes), A(child), A(parent))
+        compute_multipoles[bpg, tpb](A(pos[0]), A(pos[1]), A(pos[2]), A(mass), A(child), A(parent),
+                                     A(n_mass), A(n_com), A(n_min), A(n_max), A(counters))
+        normalize_com[(m + 255) // 256, 256](A(n_mass), A(n_com), m)
+        find_root[bpg_nodes, tpb](A(parent), A(root))
+        force.zero_()
+        node_to_cache.fill_(-1)
+        build_top_tree_cache[1, 1](A(child), A(root), A(top_nodes), A(node_to_cache), cache)
+        for off in range(0, n, batch):
+            c = min(batch, n - off)
+            compute_forces[(c + tpb - 1) // tpb, tpb](
+                A(pos[0]), A(pos[1]), A(pos[2]), A(child), A(n_mass), A(n_com), A(n_min), A(n_max),
+                A(force), cfg.THETA, cfg.G, cfg.SOFTENING, cfg.BOX_SIZE, A(root), A(top_nodes),
+                A(node_to_cache), off)
+        integrate[bpg, tpb](A(pos[0]), A(pos[1]), A(pos[2]), A(vel[0]), A(vel[1]), A(vel[2]),
+                            A(force), a, H, dt)
+        grid.zero_()
+        mvp = torch.from_numpy(get_mvp_matrix(i, (0.5, 0.5, 0.5), 1.0, cfg)).to(dev)
+        render_density[bpg, tpb](A(pos[0]), A(pos[1]), A(pos[2]), A(grid), A(mvp), res)
+        st["a"] = a + 0.002
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for i in range(args.steps):
+        step(args.warmup + i)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / args.steps
+    print(json.dumps(dict(base, value=n / (ms * 1e-3), unit="particle-steps/s", n_gpus=1,
+                          steps=args.steps, warmup=args.warmup, ms_per_step=ms, higher_is_better=True,
+                          dtype="f32 storage, f64 force arithmetic (compiled Numba)",
+                          data="synthetic (seeded Zel'dovich ICs)",
+                          config=dict(config_dict(cfg, args), splat="1024x1024 (reference square grid)",
+                                      keys="63-bit Morton (torch) in place of compute_codes' 30-bit keys",
+                                      sort="torch.argsort(stable=True) in place of cp.argsort",
+                                      force_launches_per_step=(n + batch - 1) // batch))), flush=True)
     return 0
 
 
@@ -737,6 +864,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.impl == "reference-gpu":
+        return run_reference_gpu(args)
     return run_ours(args)
 
 
