@@ -275,16 +275,25 @@ def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
                 interactions_per_body_bound=float(total / s.n))
 
 
-def _reference_tree_forces(n_grid, pos, vel, bpl):
-    """Periodic-law forces of every body with quadrupoles at theta = 0.2 (in
-    the same sorted order as an engine built on the same bodies)."""
+def _reference_tree_forces(n_grid, pos, vel, bpl, thetas=(0.2, 0.25, 0.3)):
+    """Periodic-law forces of every body with quadrupoles at the smallest
+    theta of `thetas` whose walk fits the traversal's node stack (in the same
+    sorted order as an engine built on the same bodies).  Returns (forces
+    float64 [N, 3], the engine, the theta used)."""
+    from ._lib import CnbError
     n = n_grid ** 3
-    qeng = SimulationEngine(_cfg(n_grid, MAC="ewald", QUADRUPOLE=True, THETA=0.2,
-                                 BODIES_PER_LANE=bpl, BLOCK_WARPS=4),
-                            SimulationState(n, pos, vel), camera=False)
-    qeng.forces_only()
-    qeng.check()
-    return qeng.state.force.double(), qeng
+    for th in thetas:
+        qeng = SimulationEngine(_cfg(n_grid, MAC="ewald", QUADRUPOLE=True, THETA=th,
+                                     BODIES_PER_LANE=bpl, BLOCK_WARPS=4),
+                                SimulationState(n, pos, vel), camera=False)
+        qeng.forces_only()
+        try:
+            qeng.check()
+        except CnbError:
+            del qeng
+            continue
+        return qeng.state.force.double(), qeng, th
+    raise RuntimeError("no reference theta fits the node stack")
 
 
 def _state_labels(n_grid, seed, evolve, bpl):
@@ -298,13 +307,13 @@ def _state_labels(n_grid, seed, evolve, bpl):
                            SimulationState(n, pos, vel), camera=False)
     eng.forces_only()
     acc = eng.state.force.clone()
-    ref, _ = _reference_tree_forces(n_grid, pos, vel, bpl)
+    ref, _, ref_theta = _reference_tree_forces(n_grid, pos, vel, bpl)
     b = lagrangian_bound(eng, ref)
     alloc = b.pop("theta_allocation")
     tm = eng.tree_manager
     feats = bucket_features(tm.node_table, tm.parent, tm.workspace, n, acc)
     nb = alloc.numel()
-    return feats[:nb], alloc, dict(seed=seed, buckets=nb, bound=b["bound"])
+    return feats[:nb], alloc, dict(seed=seed, buckets=nb, bound=b["bound"], reference_theta=ref_theta)
 
 
 def controller(args):
@@ -343,7 +352,7 @@ def controller(args):
     eng.forces_only()
     plain_acc = eng.state.force.clone()
     # reference-accuracy forces on every body: quadrupoles at theta = 0.2 (same sort)
-    ref_tree, qeng = _reference_tree_forces(args.n_grid, pos, vel, args.bpl)
+    ref_tree, qeng, ref_theta = _reference_tree_forces(args.n_grid, pos, vel, args.bpl)
     targets = np.sort(np.random.default_rng(0).choice(n, args.sample, replace=False)).astype(np.int64)
     ref_direct = _direct(eng.state, targets, eng.config.SOFTENING, periodic=True)
     tree_err = _errors(qeng.state.force, ref_direct, targets)
@@ -411,7 +420,8 @@ def controller(args):
                           training=dict(labels=args.labels, samples=int(y.numel()),
                                         over_weight=args.over_weight),
                           a=a, labels=info, train_loss=[curve[0], curve[-1]], train_seconds=t_train,
-                          reference_tree_vs_direct=tree_err, bound=bound, uniform_theta=curve_rows,
+                          reference_tree_theta=ref_theta, reference_tree_vs_direct=tree_err, bound=bound,
+                          uniform_theta=curve_rows,
                           plain_theta05=plain, learned=learned, learned_scale=lo,
                           gain_interactions=gain, gain_forces_ms=plain["ms"] / learned["ms"],
                           fraction_of_bound=gain / bound["bound"],

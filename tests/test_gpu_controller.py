@@ -158,3 +158,62 @@ def test_labels_and_learned_theta_gain():
     # the labels are close to uniform and the measured gain is about 0.9x
     # (no gain); the bound only guards against a broken controller.
     assert gain > 0.7, (cost_l, cost_plain, p99_l, p99_plain)
+
+
+def test_lagrangian_labels_and_gain_under_the_periodic_law():
+    """Under the periodic (Ewald) law, where theta sets the cost: labels from
+    the Lagrangian allocation of a batch of small boxes (least interactions
+    at plain theta = 0.5's p99), the network trained on them, and on a
+    held-out 48^3 box the learned angles -- scaled to plain's p99 relative
+    error against the float64 Ewald direct sum -- need fewer interactions
+    than plain theta = 0.5.  The allocation's own gain on the training
+    buckets is the bound of any per-bucket policy there."""
+    from cnb.controller import ThetaController, make_labels, direct_sum
+    from cnb.core.batched import BatchedBoxes, draw_boxes
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils import config as cfgmod
+    from cnb.utils.cosmology import zeldovich_arrays
+    train = BatchedBoxes(draw_boxes(16, seed=3, grids=(16, 24, 32)), mac="ewald", bodies_per_lane=2)
+    X, y, info = make_labels(train, per_box=512)
+    assert info["objective"] == "lagrangian"
+    assert info["violations"] <= info["allowed_violations"]
+    assert info["bound"] > 1.2
+    ctl = ThetaController(seed=0)
+    ctl.train(X, y, steps=1500, lr=3e-3, over_weight=2.0)
+    n_grid = 48
+    cfg = cfgmod.make(N_GRID=n_grid, SOFTENING=0.5 / n_grid, THETA=0.5, KEY_MODE="morton63",
+                      FORCE_MODE="grouped", MAC="ewald", BODIES_PER_LANE=2, BLOCK_WARPS=4)
+    pos, vel = zeldovich_arrays(n_grid, 77)
+    eng = SimulationEngine(cfg, SimulationState(n_grid ** 3, pos, vel), camera=False)
+    eng.forces_only()
+    acc = eng.state.force.clone()
+    s = eng.state
+    t = torch.from_numpy(np.sort(np.random.default_rng(0).choice(s.n, 1024, replace=False))).cuda()
+    ref = direct_sum(s.pos, s.mass, t, 1.0, cfg.SOFTENING, periodic=True)
+
+    def run(scale=None):
+        eng.controller = ctl if scale is not None else None
+        eng.controller_scale = scale or 1.0
+        eng.controller_accel = acc
+        if scale is None:
+            eng.theta_per_group = None
+        eng.stats.zero_()
+        eng.compute_forces()
+        e = ((s.force[t].double() - ref).norm(dim=1) / ref.norm(dim=1)).cpu().numpy()
+        return float(np.percentile(e, 99)), float(eng.stats[0].item()) / s.n
+
+    p99_plain, cost_plain = run(None)
+    lo, hi = 0.2, 3.0
+    for _ in range(14):
+        mid = 0.5 * (lo + hi)
+        p99, _ = run(mid)
+        lo, hi = (mid, hi) if p99 <= p99_plain else (lo, mid)
+    p99_l, cost_l = run(lo)
+    eng.controller = None
+    eng.check()
+    gain = cost_plain / cost_l
+    print(f"periodic law: plain p99 {p99_plain:.4g} {cost_plain:.0f}/body; learned p99 {p99_l:.4g} "
+          f"{cost_l:.0f}/body (scale {lo:.3f}); gain {gain:.3f}x; label bound {info['bound']:.3f}x")
+    assert p99_l <= p99_plain
+    assert gain > 1.15, (gain, info)
