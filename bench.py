@@ -22,10 +22,12 @@ order, sort them, merge them back) replaces the full radix sort whenever at most
 
 `--impl ours` (default) runs libcnb on the GPU; `--impl reference` times the
 reference's algorithm (the CPU oracle restating src/kernels/*.py, all host
-threads) on the same workload, each step a bounded sample (all stages on all
-bodies except the force traversal, which runs on a fixed sample of targets
-and is scaled to N).  Under torchrun each rank runs an independent box
-(seed 1 + 1000 * rank: replicas, weak scaling); rank 0 prints the JSON line.
+threads) on the same workload, every stage on every body (about 3.5 s per
+step on 16 cores; --cpu-sample K times the force traversal on K targets and
+scales it instead).  `--impl reference-gpu` launches the reference's own
+Numba kernels on the GPU (run_reference_gpu).  Under torchrun each rank runs
+an independent box (seed 1 + 1000 * rank: replicas, weak scaling); rank 0
+prints the JSON line.
 """
 from __future__ import annotations
 
@@ -88,7 +90,9 @@ def parse():
     ap.add_argument("--width", type=int, default=1920)
     ap.add_argument("--height", type=int, default=1080)
     ap.add_argument("--accuracy-sample", type=int, default=4096)
-    ap.add_argument("--cpu-sample", type=int, default=8192)
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="reference arm: force traversal on this many evenly spaced targets scaled "
+                         "to N (0: every body, no extrapolation)")
     ap.add_argument("--no-graph", dest="graph", action="store_false",
                     help="launch every kernel from Python instead of replaying a CUDA graph")
     ap.add_argument("--no-tune", action="store_true", help="skip the launch-shape autotuner")
@@ -260,7 +264,8 @@ def cpu_reference_step(pos, vel, mass, a, da, cfg, sample, threads, full_check=F
     nm, nc, lo, hi = orc.compute_multipoles(*spos, smass, ch, par)
     root = orc.find_root(par)
     t1 = time.perf_counter()
-    targets = np.linspace(0, n - 1, min(sample, n)).astype(np.int64)
+    targets = (np.linspace(0, n - 1, min(sample, n)).astype(np.int64) if sample > 0
+               else np.arange(n, dtype=np.int64))
     orc.forces_targets_f64(*spos, ch, nm, nc, lo, hi, cfg.THETA, cfg.G, cfg.SOFTENING,
                            cfg.BOX_SIZE, root, targets, nthreads=threads)
     t2 = time.perf_counter()
@@ -284,6 +289,13 @@ def cpu_reference_step(pos, vel, mass, a, da, cfg, sample, threads, full_check=F
     return new[:3], new[3:], seconds, check
 
 
+def _sample_text(sample, n):
+    if 0 < sample < n:
+        return (f"all stages on all {n} bodies; force traversal (reference per-body algorithm, "
+                f"float64) on {sample} evenly spaced targets scaled to N")
+    return f"one full step: every stage, force traversal (float64) on all {n} bodies"
+
+
 def run_reference(args):
     ws, rank, _ = int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")), 0
     if rank != 0:
@@ -305,9 +317,11 @@ def run_reference(args):
         total += s
     wall = time.perf_counter() - wall0
     value = n * args.steps / total
-    # the sampled force traversal against the traversal timed on every body, once
-    _, _, _, check = cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads,
-                                        full_check=True)
+    check = None
+    if 0 < args.cpu_sample < n:
+        # the sampled force traversal against the traversal timed on every body, once
+        _, _, _, check = cpu_reference_step(pos, vel, mass, a, 0.002, cfg, args.cpu_sample, threads,
+                                            full_check=True)
     line = {
         "impl": "reference", "metric": metric_for(args.n_grid), "value": value, "unit": "particle-steps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -315,12 +329,12 @@ def run_reference(args):
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Zel'dovich ICs)",
         "config": config_dict(cfg, args),
         "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-                         "sample": f"all stages on all {n} bodies; force traversal on {args.cpu_sample} "
-                                   f"evenly spaced targets scaled to N"},
+                         "sample": _sample_text(args.cpu_sample, n)},
         "sampling": {"timed_seconds_actual": wall,
-                     "note": "ms_per_step is the full step the sample stands for: the force traversal "
-                             "of the sampled targets scaled to all bodies (checked below against the "
-                             "traversal timed on every body of one step)",
+                     "note": ("every stage on every body, nothing extrapolated" if check is None else
+                              "ms_per_step is the full step the sample stands for: the force traversal "
+                              "of the sampled targets scaled to all bodies (checked below against the "
+                              "traversal timed on every body of one step)"),
                      "check": check},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -705,6 +719,7 @@ def learned_vs_plain(args, flush):
     targets = np.sort(np.random.default_rng(0).choice(n, args.learned_sample, replace=False)).astype(np.int64)
     t0 = time.time()
     ref = _direct(eng.state, targets, cfg.SOFTENING, periodic=True)
+    torch.cuda.synchronize()
     direct_s = time.time() - t0
     ref_self = _errors(qeng.state.force, ref, targets)
     del qeng
@@ -856,9 +871,7 @@ def cpu_baseline(args):
     threads = os.cpu_count() or 1
     _, _, s = cpu_reference_step(pos, vel, mass, cfg.A_START, 0.002, cfg, args.cpu_sample, threads)
     return {"value": n / s, "unit": "particle-steps/s", "cores": threads, "kind": "port",
-            "sample": f"one step: all stages on all {n} bodies, force traversal (reference "
-                      f"per-body algorithm, float64) on {args.cpu_sample} evenly spaced targets "
-                      f"scaled to N"}
+            "sample": _sample_text(args.cpu_sample, n)}
 
 
 def main():

@@ -124,6 +124,7 @@ def test_labels_and_learned_theta_gain():
     ctl.train(X, y, steps=1500, lr=3e-3, over_weight=4.0)
     eng = _built_engine(n_grid=32, seed=77)          # held-out box
     s = eng.state
+    eng.controller_accel = s.force.clone()           # the features' acceleration input, fixed
     t = torch.from_numpy(np.sort(np.random.default_rng(0).choice(s.n, 4096, replace=False))).cuda()
     ref = direct_sum(s.pos, s.mass, t, 1.0, eng.config.SOFTENING)
     rms = ref.norm(dim=1).pow(2).mean().sqrt()
