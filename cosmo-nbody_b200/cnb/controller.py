@@ -189,7 +189,7 @@ def allocate(errors, costs, owner, budget, allowed):
         return idx, viol[idx, np.arange(G)].sum()
 
     # with an unbounded price every bucket minimises its violations first
-    big = costs.max() * (G + 1) + 1.0
+    big = costs[np.isfinite(costs)].max() * (G + 1) + 1.0   # infinite cost: a theta never chosen
     idx_big, v_big = pick(big)
     if v_big > allowed:
         return idx_big, float(costs[idx_big, np.arange(G)].sum()), float(v_big)

@@ -246,6 +246,8 @@ def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
     costs = np.zeros((len(thetas), nb))
     saved = eng.theta_per_group, eng.controller
     eng.controller = None
+    from ._arrays import read_status
+    skipped = []
     try:
         for k, th in enumerate(thetas):
             eng.theta_per_group = torch.full((nb,), float(th), device=s.pos[0].device)
@@ -253,6 +255,10 @@ def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
             e = ((s.force.double() - ref).norm(dim=1) / refn).cpu().numpy()
             errs[k] = e[order]
             costs[k] = inter[:nb].cpu().numpy().astype(np.float64) * bk[:, 1]
+            if read_status(s.device.index) & _lib.FLAG_LIST_OVERFLOW:
+                # a walk outgrew the node stack at this theta: never chosen
+                costs[k] = np.inf
+                skipped.append(th)
     finally:
         eng.bucket_inter = None
         eng.theta_per_group, eng.controller = saved
@@ -268,6 +274,7 @@ def lagrangian_bound(eng, ref, thetas=None, quantile=99.0):
     ms = _time_forces(eng)
     eng.theta_per_group, eng.controller = saved
     return dict(bound=float(costs[k05].sum() / total), budget_rel=budget, allowed=allowed,
+                thetas_skipped_stack=skipped,
                 forces_ms_allocation=ms, theta_allocation=alloc,
                 violations=v, buckets=nb,
                 theta_hist={f"{t:.1f}": int((chosen == t).sum()) for t in thetas},

@@ -37,7 +37,9 @@
 // is applied with the per-pair minimum image, the cut and its mask.
 // Per-body items carry the band [lo, hi] around s^2 / theta^2 inside which
 // the float32 d^2 cannot decide, and flags for the per-pair image and the
-// cut, so the common item is a handful of packed operations per body pair.
+// cut, so the common item is a handful of packed operations per body pair;
+// lane j keeps item j's mask of opening bodies and the children of a round's
+// items are pushed together after them.
 //
 // Limit: the reference's 64-entry stack drops children when full
 // (physics_kernels.py:143-149).  That happens only for trees deeper than
@@ -111,8 +113,38 @@ __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *ma
         const float2 s2 = dup2(soft2);
         float2 fx = make_float2(ax[0], ax[1]), fy = make_float2(ay[0], ay[1]),
                fz = make_float2(az[0], az[1]);
-#pragma unroll 4
-        for (int j = 0; j < cnt; ++j) {
+        // eight entries at a time: loads, distances and masses first, then the
+        // inverse cubes and the accumulation in list order
+        int j = 0;
+        for (; j + 8 <= cnt; j += 8) {
+            float2 dx[8], dy[8], dz[8], w[8], q[8];
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const float4 a = list[2 * (j + u)], b = list[2 * (j + u) + 1];
+                const uint2 mk = masks[j + u];
+                dx[u] = __fadd2_rn(make_float2(a.x, a.y), nx);
+                dy[u] = __fadd2_rn(make_float2(a.z, a.w), ny);
+                dz[u] = __fadd2_rn(make_float2(b.x, b.y), nz);
+                if (WRAP_CUT) {
+                    dx[u] = minus_image2(dx[u]);
+                    dy[u] = minus_image2(dy[u]);
+                    dz[u] = minus_image2(dz[u]);
+                }
+                q[u] = __ffma2_rn(dx[u], dx[u], __ffma2_rn(dy[u], dy[u], __ffma2_rn(dz[u], dz[u], s2)));
+                const bool u0 = (mk.x >> lane) & 1u, u1 = (mk.y >> lane) & 1u;
+                w[u] = make_float2(u0 && (!WRAP_CUT || q[u].x > cut) ? b.z : 0.f,
+                                   u1 && (!WRAP_CUT || q[u].y > cut) ? b.w : 0.f);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const float2 r = make_float2(rsqrtf(q[u].x), rsqrtf(q[u].y));
+                const float2 f = __fmul2_rn(__fmul2_rn(__fmul2_rn(w[u], r), r), r);
+                fx = __ffma2_rn(f, dx[u], fx);
+                fy = __ffma2_rn(f, dy[u], fy);
+                fz = __ffma2_rn(f, dz[u], fz);
+            }
+        }
+        for (; j < cnt; ++j) {
             const float4 a = list[2 * j], b = list[2 * j + 1];
             const uint2 mk = masks[j];
             float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx);
@@ -169,7 +201,7 @@ __device__ __forceinline__ void per_body_item(float4 I, float4 J, uint32_t m0, u
                                               double th2d, float soft2, const float (&x)[BPL],
                                               const float (&y)[BPL], const float (&z)[BPL],
                                               float (&ax)[BPL], float (&ay)[BPL], float (&az)[BPL],
-                                              bool (&opn)[BPL], int &n_acc) {
+                                              bool (&opn)[BPL]) {
     const int flags = __float_as_int(J.w);
     if constexpr (BPL == 2) {
         float2 dx = __fadd2_rn(dup2(I.x), make_float2(-x[0], -x[1]));
@@ -188,7 +220,6 @@ __device__ __forceinline__ void per_body_item(float4 I, float4 J, uint32_t m0, u
         const bool u0 = in0 && a0, u1 = in1 && a1;
         opn[0] = in0 && !a0;
         opn[BPL - 1] = in1 && !a1;
-        n_acc += (int)u0 + (int)u1;
         bool f0 = u0, f1 = u1;
         if (flags & kItemNear) {
             f0 = f0 && ref_outside_cut(dx.x, dy.x, dz.x, d2.x);
@@ -219,7 +250,6 @@ __device__ __forceinline__ void per_body_item(float4 I, float4 J, uint32_t m0, u
             if (in && !a && !(d2 < J.y)) a = ref_accepts_f64(J.x, th2d, dx, dy, dz);
             const bool u = in && a;
             opn[b] = in && !a;
-            n_acc += (int)u;
             const bool fu = u && (!(flags & kItemNear) || ref_outside_cut(dx, dy, dz, d2));
             const float r = rsqrtf(d2 + soft2);
             const float f = fu ? I.w * r * r * r : 0.f;
@@ -499,37 +529,53 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                                                __uint_as_float(mk.x), __uint_as_float(mk.y));
             }
             __syncwarp();
-            // per-body items: every body of the mask decides for itself
+            // per-body items: every body of the mask decides for itself; lane j
+            // keeps item j's mask of opening bodies, and the children of every
+            // item that some body opened are pushed together afterwards
+            uint2 my_om = make_uint2(0u, 0u);
+#pragma unroll 2
             for (int j = 0; j < pcnt; ++j) {
                 const float4 I = plist[3 * j], J = plist[3 * j + 1], K = plist[3 * j + 2];
                 bool opn[BPL];
                 per_body_item<BPL>(I, J, __float_as_uint(K.z), __float_as_uint(K.w), lane, th2d, soft2,
-                                   x, y, z, ax, ay, az, opn, n_acc);
-                const uint2 om = make_uint2(__ballot_sync(0xffffffffu, opn[0]),
-                                            BPL == 2 ? __ballot_sync(0xffffffffu, opn[BPL - 1]) : 0u);
-                if (om.x | om.y) {
-                    const int32_t k0 = __float_as_int(K.x), k1c = __float_as_int(K.y);
-                    if (om.x == fm.x && om.y == fm.y) {
-                        if (top + 2 > kGStack) {
-                            overflow = true;
-                        } else {
-                            if (lane == 0) {
-                                stack[top] = k1c;
-                                stack[top + 1] = k0;
-                            }
-                            top += 2;
-                        }
-                    } else if (ptop + 2 > kXPStack) {
-                        overflow = true;
-                    } else {
-                        if (lane == 0) {
-                            pstack[ptop] = k1c;
-                            pstack[ptop + 1] = k0;
-                            psmask[ptop] = om;
-                            psmask[ptop + 1] = om;
-                        }
-                        ptop += 2;
+                                   x, y, z, ax, ay, az, opn);
+                const uint32_t o0 = __ballot_sync(0xffffffffu, opn[0]);
+                const uint32_t o1 = BPL == 2 ? __ballot_sync(0xffffffffu, opn[BPL - 1]) : 0u;
+                if (lane == j) my_om = make_uint2(o0, o1);
+            }
+            if (pcnt > 0) {
+                bool has = false, whole_o = false;
+                int32_t k0 = -1, k1c = -1;
+                if (lane < pcnt) {
+                    const float4 K = plist[3 * lane + 2];
+                    k0 = __float_as_int(K.x);
+                    k1c = __float_as_int(K.y);
+                    has = (my_om.x | my_om.y) != 0u;
+                    whole_o = my_om.x == fm.x && my_om.y == fm.y;
+                    // the bodies of the item's mask that did not open it accepted it
+                    n_acc += __popc(__float_as_uint(K.z)) + __popc(__float_as_uint(K.w)) -
+                             __popc(my_om.x) - __popc(my_om.y);
+                }
+                const uint32_t mw = __ballot_sync(0xffffffffu, has && whole_o);
+                const uint32_t mp = __ballot_sync(0xffffffffu, has && !whole_o);
+                const int nw = __popc(mw), npart = __popc(mp);
+                if (top + 2 * nw > kGStack || ptop + 2 * npart > kXPStack) {
+                    overflow = true;  // children dropped (flagged)
+                } else {
+                    if (has && whole_o) {
+                        const int pos = top + 2 * __popc(mw & lt);
+                        stack[pos] = k1c;
+                        stack[pos + 1] = k0;
                     }
+                    if (has && !whole_o) {
+                        const int pos = ptop + 2 * __popc(mp & lt);
+                        pstack[pos] = k1c;
+                        pstack[pos + 1] = k0;
+                        psmask[pos] = my_om;
+                        psmask[pos + 1] = my_om;
+                    }
+                    top += 2 * nw;
+                    ptop += 2 * npart;
                 }
             }
             max_top = max(max_top, top + ptop);
