@@ -6,8 +6,10 @@
 // theta = THETA_LO + (THETA_HI - THETA_LO) * sigmoid(z), i.e. clipped to
 // [0.2, 1.0].  Parameters (CNB_MLP_PARAMS floats, this order):
 //   W1[64][12], b1[64], W2[64][64], b2[64], w3[64], b3.
-// Inference keeps the weights in bfloat16 and accumulates in float32;
-// training keeps float32 master weights.
+// Inference keeps the weights in bfloat16 and accumulates in float32: the
+// first layer in float32 per bucket, the 64 x 64 second layer on the tensor
+// cores (mma.sync m16n8k16, its input -- the first layer's SiLU outputs --
+// rounded to bfloat16); training keeps float32 master weights.
 //
 // Features of a bucket (its subtree node v, ancestors p1..p3), lengths in
 // units of the box's mean body spacing s = (body mass)^(1/3):
@@ -128,65 +130,124 @@ __device__ __forceinline__ float theta_of(float z) {
     return kThetaLo + (kThetaHi - kThetaLo) * sigmoidf_(z);
 }
 
-// Fused inference, one warp per bucket: the lanes read the bucket's
-// accelerations (coalesced) and form its features, then the network with
-// the bfloat16 weights converted once per block into float32 shared memory
-// (W2 transposed so that lane k reads row k of every column): lane j owns
-// hidden units j and j + 32 of both layers, the output is a warp sum.
-constexpr int kCtlWarps = 8;
-__global__ void __launch_bounds__(kCtlWarps * 32) k_controller(const float4 *__restrict__ rec,
-                                                             const float4 *__restrict__ aabb,
-                                                             const int32_t *__restrict__ parents,
-                                                             const int32_t *__restrict__ ws,
-                                                             const float *__restrict__ accel,
-                                                             const uint32_t *__restrict__ perm,
-                                                             const __nv_bfloat16 *__restrict__ wbf,
-                                                             float *__restrict__ theta, int max_buckets) {
-    __shared__ float w[kParams];
-    __shared__ float hbuf[kCtlWarps][kH];
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
-        int dst = i;
-        if (i >= kOffW2 && i < kOffB2) {
-            const int k = (i - kOffW2) / kH, j = (i - kOffW2) % kH;  // W2[k][j]
-            dst = kOffW2 + j * kH + k;
-        }
-        w[dst] = __bfloat162float(wbf[i]);
+// Fused inference with the 64 x 64 hidden layer on the tensor cores: one
+// warp takes 32 buckets (two 16-row tiles).  Each lane forms one bucket's
+// features and its first layer in float32 (12 -> 64, SiLU) and stores the
+// hidden vector as bfloat16 in shared memory; the second layer is
+// mma.sync.m16n8k16 (bf16 inputs, float32 accumulation) against W2 in
+// bfloat16; bias, SiLU and the output layer are applied on the accumulator
+// fragments and summed over the four lanes that share a row.
+constexpr int kMmaWarps = 4;
+constexpr int kHPad = kH + 8;  // bf16 per row of the hidden tiles: staggers the banks
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const uint32_t (&a)[4],
+                                               const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
+        "{%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, {%0, %1, %2, %3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__global__ void __launch_bounds__(kMmaWarps * 32) k_controller_mma(
+    const float4 *__restrict__ rec, const float4 *__restrict__ aabb,
+    const int32_t *__restrict__ parents, const int32_t *__restrict__ ws,
+    const float *__restrict__ accel, const uint32_t *__restrict__ perm,
+    const __nv_bfloat16 *__restrict__ wbf, float *__restrict__ theta, int max_buckets) {
+    // float32: W1, b1, b2, w3, b3; bfloat16: W2 rows (output unit) of kHPad
+    __shared__ float w1[kH * kIn], b1[kH], b2[kH], w3[kH];
+    __shared__ float b3;
+    __shared__ __align__(16) __nv_bfloat16 w2[kH * kHPad];
+    __shared__ __align__(16) __nv_bfloat16 hid[kMmaWarps][32 * kHPad];
+    for (int i = threadIdx.x; i < kH * kIn; i += blockDim.x) w1[i] = __bfloat162float(wbf[kOffW1 + i]);
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+        b1[i] = __bfloat162float(wbf[kOffB1 + i]);
+        b2[i] = __bfloat162float(wbf[kOffB2 + i]);
+        w3[i] = __bfloat162float(wbf[kOffW3 + i]);
     }
+    for (int i = threadIdx.x; i < kH * kH; i += blockDim.x) w2[(i / kH) * kHPad + i % kH] = wbf[kOffW2 + i];
+    if (threadIdx.x == 0) b3 = __bfloat162float(wbf[kOffB3]);
     __syncthreads();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
     const int nb = min(ws[0], max_buckets);
     const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
-    for (int g = blockIdx.x * kCtlWarps + wib; g < nb; g += gridDim.x * kCtlWarps) {
-        const int4 bk = buckets[g];
-        float asum = 0.f;
-        for (int k = lane; k < bk.y; k += 32) {
-            const int64_t i = (int64_t)bk.x + k;
-            const int64_t r = perm ? (int64_t)perm[i] : i;
-            const float ax = accel[3 * r], ay = accel[3 * r + 1], az = accel[3 * r + 2];
-            asum += sqrtf(ax * ax + ay * ay + az * az);
-        }
-        for (int o = 16; o > 0; o >>= 1) asum += __shfl_xor_sync(0xffffffffu, asum, o);
-        float f[kIn];
-        bucket_features(rec, aabb, parents, asum / (float)bk.y, bk, f);
+    __nv_bfloat16 *h = hid[wib];
+    for (int base = (blockIdx.x * kMmaWarps + wib) * 32; base < nb; base += gridDim.x * kMmaWarps * 32) {
+        // one bucket per lane: features and the first layer in float32
+        const int g = base + lane;
+        if (g < nb) {
+            const int4 bk = buckets[g];
+            float f[kIn];
+            bucket_features(rec, aabb, parents, bucket_mean_accel(accel, perm, bk), bk, f);
+#pragma unroll 4
+            for (int j = 0; j < kH; j += 2) {
+                float a0 = b1[j], a1 = b1[j + 1];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
-            const int j = lane + 32 * u;
-            float a = w[kOffB1 + j];
-#pragma unroll
-            for (int i = 0; i < kIn; ++i) a = fmaf(w[kOffW1 + j * kIn + i], f[i], a);
-            hbuf[wib][j] = siluf_(a);
+                for (int i = 0; i < kIn; ++i) {
+                    a0 = fmaf(w1[j * kIn + i], f[i], a0);
+                    a1 = fmaf(w1[(j + 1) * kIn + i], f[i], a1);
+                }
+                *reinterpret_cast<uint32_t *>(h + lane * kHPad + j) = pack_bf16(siluf_(a0), siluf_(a1));
+            }
+        } else {
+            for (int j = 0; j < kH; j += 2) *reinterpret_cast<uint32_t *>(h + lane * kHPad + j) = 0u;
         }
         __syncwarp();
-        float a0 = w[kOffB2 + lane], a1 = w[kOffB2 + lane + 32];
-#pragma unroll 8
-        for (int j = 0; j < kH; ++j) {
-            const float h = hbuf[wib][j];
-            a0 = fmaf(w[kOffW2 + j * kH + lane], h, a0);
-            a1 = fmaf(w[kOffW2 + j * kH + lane + 32], h, a1);
+        // second layer: rows = buckets, columns = hidden units, k = first-layer units
+        float z[2][2] = {{0.f, 0.f}, {0.f, 0.f}};  // [m tile][row gid / gid + 8]
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            uint32_t a[4][4];
+            const __nv_bfloat16 *r0 = h + (mt * 16 + gid) * kHPad, *r1 = r0 + 8 * kHPad;
+#pragma unroll
+            for (int kt = 0; kt < 4; ++kt) {
+                const int c = kt * 16 + tig * 2;
+                a[kt][0] = *reinterpret_cast<const uint32_t *>(r0 + c);
+                a[kt][1] = *reinterpret_cast<const uint32_t *>(r1 + c);
+                a[kt][2] = *reinterpret_cast<const uint32_t *>(r0 + c + 8);
+                a[kt][3] = *reinterpret_cast<const uint32_t *>(r1 + c + 8);
+            }
+#pragma unroll
+            for (int nt = 0; nt < kH / 8; ++nt) {
+                float d[4] = {0.f, 0.f, 0.f, 0.f};
+                const __nv_bfloat16 *wr = w2 + (nt * 8 + gid) * kHPad;  // output unit nt*8 + gid
+#pragma unroll
+                for (int kt = 0; kt < 4; ++kt) {
+                    const int c = kt * 16 + tig * 2;
+                    const uint32_t b[2] = {*reinterpret_cast<const uint32_t *>(wr + c),
+                                           *reinterpret_cast<const uint32_t *>(wr + c + 8)};
+                    mma_bf16_16816(d, a[kt], b);
+                }
+                const int col = nt * 8 + tig * 2;
+                z[mt][0] = fmaf(w3[col], siluf_(d[0] + b2[col]), z[mt][0]);
+                z[mt][0] = fmaf(w3[col + 1], siluf_(d[1] + b2[col + 1]), z[mt][0]);
+                z[mt][1] = fmaf(w3[col], siluf_(d[2] + b2[col]), z[mt][1]);
+                z[mt][1] = fmaf(w3[col + 1], siluf_(d[3] + b2[col + 1]), z[mt][1]);
+            }
         }
-        float z = fmaf(w[kOffW3 + lane], siluf_(a0), w[kOffW3 + lane + 32] * siluf_(a1));
-        for (int o = 16; o > 0; o >>= 1) z += __shfl_xor_sync(0xffffffffu, z, o);
-        if (lane == 0) theta[g] = theta_of(z + w[kOffB3]);
+        // the four lanes of a row group hold its partial sums
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                z[mt][q] += __shfl_xor_sync(0xffffffffu, z[mt][q], 1);
+                z[mt][q] += __shfl_xor_sync(0xffffffffu, z[mt][q], 2);
+            }
+        if (tig == 0) {
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    const int gg = base + mt * 16 + gid + 8 * q;
+                    if (gg < nb) theta[gg] = theta_of(z[mt][q] + b3);
+                }
+        }
         __syncwarp();
     }
 }
@@ -374,9 +435,10 @@ extern "C" int cnb_controller_theta(const float *node_table, const int32_t *pare
         return CNB_E_INVALID_ARG;
     const int64_t m = 2 * n - 1;
     const float4 *rec = reinterpret_cast<const float4 *>(node_table);
-    k_controller<<<grid_for(max_buckets, kCtlWarps, 148 * 8), kCtlWarps * 32, 0, as_stream(stream)>>>(
-        rec, rec + 2 * m, parents, workspace, accel, perm,
-        reinterpret_cast<const __nv_bfloat16 *>(weights_bf16), theta, max_buckets);
+    k_controller_mma<<<grid_for(max_buckets, kMmaWarps * 32, 148 * 4), kMmaWarps * 32, 0,
+                       as_stream(stream)>>>(rec, rec + 2 * m, parents, workspace, accel, perm,
+                                            reinterpret_cast<const __nv_bfloat16 *>(weights_bf16),
+                                            theta, max_buckets);
     return launch_status();
 }
 

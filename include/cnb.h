@@ -461,8 +461,10 @@ int cnb_bucket_features(const float *node_table, const int32_t *parents,
                         const uint32_t *perm, float *features, int max_buckets, void *stream);
 
 /* Fused inference: features and the network (bfloat16 weights, float32
- * accumulation) -> theta per bucket slot, the theta_per_bucket input of
- * cnb_forces_grouped (accel, perm as for cnb_bucket_features). */
+ * accumulation; the 64 x 64 layer on the tensor cores with the first layer's
+ * outputs rounded to bfloat16) -> theta per bucket slot, the
+ * theta_per_bucket input of cnb_forces_grouped (accel, perm as for
+ * cnb_bucket_features). */
 int cnb_controller_theta(const float *node_table, const int32_t *parents,
                          const int32_t *workspace, int64_t n, const float *accel,
                          const uint32_t *perm, const void *weights_bf16, float *theta,

@@ -44,11 +44,16 @@ def dsilu(x):
     return s * (1.0 + x * (1.0 - s))
 
 
-def forward(p, X):
+def forward(p, X, hidden_bf16=False):
+    """theta and the activations; hidden_bf16: round the first layer's SiLU
+    outputs to bfloat16, as the fused inference kernel feeds them to the
+    tensor cores."""
     W1, b1, W2, b2, w3, b3 = unpack(p)
     X = np.asarray(X, np.float64)
     a1 = X @ W1.T + b1
     h1 = silu(a1)
+    if hidden_bf16:
+        h1 = bf16_round(h1.astype(np.float32)).astype(np.float64)
     a2 = h1 @ W2.T + b2
     h2 = silu(a2)
     z = h2 @ w3 + b3

@@ -92,8 +92,11 @@ def test_features_and_fused_inference_match_oracle():
     th = ctl.theta_for_buckets(tm.node_table, tm.parent, tm.workspace, n, acc,
                                perm)[:feats.shape[0]].cpu().numpy()
     folded = mlp.bf16_round(ctl.folded_params().cpu().numpy())
-    wth, _ = mlp.forward(folded, feats)
+    wth, _ = mlp.forward(folded, feats, hidden_bf16=True)
     np.testing.assert_allclose(th, wth, rtol=0, atol=2e-4)
+    # the float32-hidden network differs only by that rounding
+    wth32, _ = mlp.forward(folded, feats)
+    assert np.abs(th - wth32).max() < 5e-3
 
 
 def test_training_fits_a_smooth_target():
