@@ -81,6 +81,7 @@ SIGNATURES = {
     "cnb_pack_nodes": (_int, [_p, _p, _p, _p, _p, _p, _i64, _p]),
     "cnb_build_tree_ranges": (_int, [_p, _p, _p, _p, _i64, _p]),
     "cnb_make_buckets": (_int, [_p, _p, _i64, _int, _p, _p]),
+    "cnb_build_tree_buckets": (_int, [_p, _p, _p, _p, _p, _p, _i64, _int, _p, _int, _p, _p]),
     "cnb_forces_grouped": (_int, [_p, _p, _p, _p, _p, _p, _i64, _d, _p, _int, _int, _int, _d, _d, _d,
                                   _d, _p, _p, _p]),
     "cnb_two_level_workspace_bytes": (_i64, [_i64, _int]),

@@ -104,6 +104,7 @@ class SimulationEngine:
         super_bodies = int(super_bodies)
         if super_bodies == 0:
             self.super_bodies, self.super_ws = 0, None
+            self.tree_manager.set_super_table(None, 0)
             return
         if self.force_mode != "grouped" or self.mac not in (_lib.MAC_REF_X, _lib.MAC_REF_X_BUCKET):
             raise ValueError("SUPER_BODIES needs FORCE_MODE 'grouped' and MAC 'ref_x' or 'ref_x_bucket'")
@@ -114,6 +115,8 @@ class SimulationEngine:
             self.super_ws = torch.empty((nbytes + 15) // 16, 4, dtype=torch.int32,
                                         device=self.state.device)
         self.super_bodies = super_bodies
+        # the tree build makes the super-bucket table too
+        self.tree_manager.set_super_table(self.super_ws, super_bodies)
 
     def _stream(self):
         return int(torch.cuda.current_stream(self.state.device).cuda_stream)
@@ -160,8 +163,12 @@ class SimulationEngine:
                           self.stats.data_ptr(), status, st)
                 return
             if self.super_ws is not None and tpg is None:
+                # NULL ranges and parents: the super-bucket table was built with the tree
+                # (otherwise, e.g. after a change of super_bodies, the call builds it)
+                built = tm.super_table_current
                 _lib.call("cnb_forces_two_level", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
-                          tm.node_table.data_ptr(), tm.ranges.data_ptr(), tm.parent.data_ptr(),
+                          tm.node_table.data_ptr(), None if built else tm.ranges.data_ptr(),
+                          None if built else tm.parent.data_ptr(),
                           tm.workspace.data_ptr(), self.super_ws.data_ptr(),
                           self.super_ws.numel() * 4, self.super_bodies, s.force.data_ptr(), s.n,
                           float(cfg.THETA), self.mac, self.bodies_per_lane, self.block_warps, float(cfg.G),

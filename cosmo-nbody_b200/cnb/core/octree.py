@@ -58,15 +58,58 @@ class OctreeManager:
         self.quad = torch.zeros((m, 8), dtype=torch.float32, device=dev) if quad else None
         if quad and (not node_table or upward != "plain"):
             raise ValueError("quad needs node_table=True and the plain upward pass")
+        self.super_ws, self.super_bodies = None, 0
+        self._super_built = None
 
     def _stream(self):
         return int(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def set_super_table(self, super_ws, super_bodies):
+        """Also build the super-bucket table (super-buckets of at most
+        `super_bodies` bodies) into `super_ws` with every tree, for the
+        two-level walk; (None, 0) stops it."""
+        self.super_ws = super_ws
+        self.super_bodies = int(super_bodies) if super_ws is not None else 0
+        self._super_built = None   # made by the next build
+
+    @property
+    def _fused_build(self):
+        # tree, buckets and root in one launch, then the bucketed upward pass
+        return self.node_table is not None and self.upward == "plain" and self.bucket <= 64
+
+    @property
+    def super_table_current(self):
+        """True when `super_ws` holds the super-bucket table of the current tree
+        for the current `super_bodies` (made by the last build)."""
+        return (self.super_ws is not None and
+                self._super_built == (self.super_ws.data_ptr(), self.super_bodies))
 
     def build(self, pos_d, mass_d, codes_d):
         """octree.py:45-83: reset, build_tree, compute_multipoles, normalize_com, find_root."""
         st = self._stream()
         n, m = self.n, self.n_nodes
         status = status_buffer(self.device.index).data_ptr()
+        px, py, pz = pos_d
+        if self._fused_build:
+            # one launch builds the tree, its ranges, the bucket tables and the root index
+            # and zeroes the climb counters (leaf children and the root's parent keep the -1
+            # they were allocated with); then sums, boxes and the traversal table bucket by
+            # bucket and above the buckets; com stays raw
+            _lib.call("cnb_build_tree_buckets", codes_d.data_ptr(), self.child.data_ptr(),
+                      self.parent.data_ptr(), self.ranges.data_ptr(), self.counters.data_ptr(),
+                      self.root_idx.data_ptr(), n, self.bucket, self.workspace.data_ptr(),
+                      self.super_bodies, self.super_ws.data_ptr() if self.super_ws is not None else None,
+                      st)
+            _lib.call("cnb_upward_table_buckets", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
+                      mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
+                      self.workspace.data_ptr(), self.counters.data_ptr(),
+                      self.node_table.data_ptr(), self.sums.data_ptr(),
+                      self.quad.data_ptr() if self.quad is not None else None, n, status, st)
+            self._stale_ref = True
+            self._super_built = ((self.super_ws.data_ptr(), self.super_bodies)
+                                 if self.super_ws is not None else None)
+            return self.root_idx
+        self._super_built = None
         _lib.call("cnb_reset_tree_buffers", self.child.data_ptr(), self.parent.data_ptr(),
                   self.counters.data_ptr(), self.root_idx.data_ptr(), m, st)
         if self.node_table is not None:
@@ -74,20 +117,6 @@ class OctreeManager:
                       self.parent.data_ptr(), self.ranges.data_ptr(), n, st)
         else:
             _lib.call("cnb_build_tree", codes_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(), n, st)
-        px, py, pz = pos_d
-        if self.node_table is not None and self.upward == "plain" and self.bucket <= 64:
-            # buckets first (ranges and parents suffice), then sums, boxes and the
-            # traversal table bucket by bucket and above the buckets; com stays raw
-            _lib.call("cnb_make_buckets", self.ranges.data_ptr(), self.parent.data_ptr(), n,
-                      self.bucket, self.workspace.data_ptr(), st)
-            _lib.call("cnb_upward_table_buckets", px.data_ptr(), py.data_ptr(), pz.data_ptr(),
-                      mass_d.data_ptr(), self.child.data_ptr(), self.parent.data_ptr(),
-                      self.workspace.data_ptr(), self.counters.data_ptr(),
-                      self.node_table.data_ptr(), self.sums.data_ptr(),
-                      self.quad.data_ptr() if self.quad is not None else None, n, status, st)
-            self._stale_ref = True
-            _lib.call("cnb_find_root", self.parent.data_ptr(), self.root_idx.data_ptr(), m, st)
-            return self.root_idx
         if self.node_table is not None and self.upward == "plain":
             # one pass: sums, boxes and the traversal table; com stays raw until asked for
             if self.quad is not None:

@@ -225,6 +225,8 @@ __device__ __forceinline__ void per_body_item(float4 I, float4 J, uint32_t m0, u
             f0 = f0 && ref_outside_cut(dx.x, dy.x, dz.x, d2.x);
             f1 = f1 && ref_outside_cut(dx.y, dy.y, dz.y, d2.y);
         }
+        // an item every reaching body opens adds no force (a third of them)
+        if (!__any_sync(0xffffffffu, f0 || f1)) return;
         const float2 q = __fadd2_rn(d2, dup2(soft2));
         const float2 r = make_float2(rsqrtf(q.x), rsqrtf(q.y));
         const float2 w = make_float2(f0 ? I.w : 0.f, f1 ? I.w : 0.f);

@@ -567,7 +567,12 @@ __global__ void __launch_bounds__(kSWarps * 32) k_super_lists(SuperParams P) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     const uint32_t lt = (1u << lane) - 1u;
     int32_t *stack = stacks[wib];
-    const int n_sup = P.sws[0];
+    const int64_t n_bodies = (P.m_nodes + 1) / 2;
+    int n_sup = P.sws[0];
+    if (n_sup < 0 || n_sup > n_bodies) {  // not a super-bucket table of this tree
+        if (blockIdx.x == 0 && threadIdx.x == 0) set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
+        n_sup = 0;
+    }
     unsigned long long n_tests = 0;
     for (;;) {
         int s = 0;
@@ -575,6 +580,11 @@ __global__ void __launch_bounds__(kSWarps * 32) k_super_lists(SuperParams P) {
         s = __shfl_sync(0xffffffffu, s, 0);
         if (s >= n_sup) break;
         const int4 sb = P.supers[s];
+        if (sb.x < 0 || sb.y < 1 || (int64_t)sb.x + sb.y > n_bodies || sb.z < 0 ||
+            sb.z >= P.m_nodes) {
+            if (lane == 0) set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
+            continue;
+        }
         const bool listed = s < P.max_listed;
         for (int k = lane; k < sb.y; k += 32) P.super_of_body[sb.x + k] = listed ? s : -1;
         if (!listed) continue;
@@ -892,8 +902,10 @@ extern "C" int cnb_forces_two_level(const float *px, const float *py, const floa
     CNB_TRY(grouped_common(P, px, py, pz, node_table, workspace, force, n, nullptr, mac,
                            bodies_per_lane, block_warps, G, stats, status));
     if (n == 0) return CNB_OK;
+    // NULL ranges and parents: super_ws already holds this tree's super-bucket table
+    const bool table_built = !ranges && !parents;
     if (!super_ws || (reinterpret_cast<uintptr_t>(super_ws) & 15) || super_bodies < 32 ||
-        (n > 1 && (!ranges || !parents)))
+        (n > 1 && !table_built && (!ranges || !parents)))
         return CNB_E_INVALID_ARG;
     const int64_t fixed = two_level_fixed_bytes(n);
     if (super_ws_bytes < fixed + two_level_slot_bytes()) return CNB_E_INVALID_ARG;
@@ -914,7 +926,7 @@ extern "C" int cnb_forces_two_level(const float *px, const float *py, const floa
     int32_t *near = reinterpret_cast<int32_t *>(base + 16 + 16 * n + 16 * slots + align16(4 * n));
     float4 *far = reinterpret_cast<float4 *>(reinterpret_cast<unsigned char *>(near) +
                                              4LL * kNearCap * slots);
-    CNB_TRY(cnb_make_buckets(ranges, parents, n, super_bodies, sws, stream));
+    if (!table_built) CNB_TRY(cnb_make_buckets(ranges, parents, n, super_bodies, sws, stream));
 
     SuperParams S{};
     S.rec = P.rec;

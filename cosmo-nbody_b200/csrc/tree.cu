@@ -32,6 +32,63 @@ __device__ __forceinline__ int delta_fn(const uint64_t *__restrict__ codes, uint
     return __clzll((long long)(ki ^ kj));
 }
 
+// delta_fn with 32-bit indices (n <= 2^29, so i + 2 n stays below 2^31):
+// the same values; for i != j, 63 - clz64(i ^ j) = 31 - clz32(i ^ j), and
+// i == j gives 63 in both forms.
+__device__ __forceinline__ int delta_fn32(const uint64_t *__restrict__ codes, uint64_t ki, int i,
+                                          int j, int n) {
+    if ((unsigned)j >= (unsigned)n) return -1;
+    const uint64_t kj = __ldg(codes + j);
+    if (ki == kj) return 64 + (31 - __clz(i ^ j));
+    return __clzll((long long)(ki ^ kj));
+}
+
+// tree_kernels.py:60-129: the range [lo, hi] of split i's node, its split
+// position gamma and its two children.  I: int64_t, or int for n <= 2^29
+// (the same search, half the instructions).
+struct Split {
+    int64_t lo, hi, gamma;
+    int32_t c0, c1;
+};
+
+template <typename I>
+__device__ __forceinline__ int delta_any(const uint64_t *__restrict__ codes, uint64_t ki, I i, I j,
+                                         I n) {
+    if constexpr (sizeof(I) == 4) return delta_fn32(codes, ki, i, j, n);
+    else return delta_fn(codes, ki, i, j, n);
+}
+
+template <typename I>
+__device__ __forceinline__ Split split_of(const uint64_t *__restrict__ codes, I i, I n) {
+    const uint64_t ki = __ldg(codes + i);
+    const int d_prev = delta_any<I>(codes, ki, i, i - 1, n);
+    const int d_next = delta_any<I>(codes, ki, i, i + 1, n);
+    const I dir = d_next > d_prev ? 1 : -1;
+    const int min_delta = d_next > d_prev ? d_prev : d_next;
+    I l_max = 2;
+    while (delta_any<I>(codes, ki, i, i + l_max * dir, n) > min_delta) l_max *= 2;
+    I l = 0;
+    for (I t = l_max >> 1; t >= 1; t >>= 1)  // t > 0: the reference's t // 2
+        if (delta_any<I>(codes, ki, i, i + (l + t) * dir, n) > min_delta) l += t;
+    const I j = i + l * dir;
+    const int delta_node = delta_any<I>(codes, ki, i, j, n);
+    I s = 0;
+    for (I t = l; t > 0;) {
+        I step = (t + 1) >> 1;
+        if (delta_any<I>(codes, ki, i, i + (s + step) * dir, n) > delta_node) s += step;
+        t -= step;
+    }
+    Split r;
+    I gamma = i + s * dir;
+    if (dir == -1) gamma -= 1;
+    r.gamma = gamma;
+    r.lo = i < j ? i : j;
+    r.hi = i < j ? j : i;
+    r.c0 = (int32_t)(r.lo == r.gamma ? r.gamma : r.gamma + n);
+    r.c1 = (int32_t)(r.hi == r.gamma + 1 ? r.gamma + 1 : r.gamma + 1 + n);
+    return r;
+}
+
 // tree_kernels.py:60-129 build_tree, one thread per split i < n-1.
 __global__ void __launch_bounds__(256) k_build_tree(const uint64_t *__restrict__ codes,
                                                     int32_t *__restrict__ children,
@@ -39,44 +96,33 @@ __global__ void __launch_bounds__(256) k_build_tree(const uint64_t *__restrict__
                                                     int2 *__restrict__ ranges) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n - 1;
          i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t ki = __ldg(codes + i);
+        const Split q = split_of<int64_t>(codes, i, n);
         const int64_t idx = i + n;
-        const int d_prev = delta_fn(codes, ki, i, i - 1, n);
-        const int d_next = delta_fn(codes, ki, i, i + 1, n);
-        const int64_t dir = d_next > d_prev ? 1 : -1;
-        const int min_delta = d_next > d_prev ? d_prev : d_next;
-        int64_t l_max = 2;
-        while (delta_fn(codes, ki, i, i + l_max * dir, n) > min_delta) l_max *= 2;
-        int64_t l = 0;
-        for (int64_t t = l_max / 2; t >= 1; t /= 2)
-            if (delta_fn(codes, ki, i, i + (l + t) * dir, n) > min_delta) l += t;
-        const int64_t j = i + l * dir;
-        const int delta_node = delta_fn(codes, ki, i, j, n);
-        int64_t s = 0;
-        for (int64_t t = l; t > 0;) {
-            int64_t step = (t + 1) / 2;
-            if (delta_fn(codes, ki, i, i + (s + step) * dir, n) > delta_node) s += step;
-            t -= step;
-        }
-        int64_t gamma = i + s * dir;
-        if (dir == -1) gamma -= 1;
-        const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
-        const int32_t c0 = (int32_t)(lo == gamma ? gamma : gamma + n);
-        const int32_t c1 = (int32_t)(hi == gamma + 1 ? gamma + 1 : gamma + 1 + n);
-        children[2 * idx] = c0;
-        children[2 * idx + 1] = c1;
-        parents[c0] = (int32_t)idx;
-        parents[c1] = (int32_t)idx;
-        if (ranges) ranges[i] = make_int2((int)lo, (int)hi);
+        children[2 * idx] = q.c0;
+        children[2 * idx + 1] = q.c1;
+        parents[q.c0] = (int32_t)idx;
+        parents[q.c1] = (int32_t)idx;
+        if (ranges) ranges[i] = make_int2((int)q.lo, (int)q.hi);
     }
+}
+
+// The bodies' (index + 1) summed over a bucket, modulo 2^32.  Summed over a
+// bucket table it is n (n + 1) / 2 when the buckets tile the bodies once; a
+// body in no bucket or in two moves it.  The bucketed upward pass checks it,
+// and checks the topology inside every bucket: the reference's tie rule for
+// equal keys (64 + 63 - clz(i ^ j), larger for farther indices) can build a
+// tree in which some node has no parent and another has two.
+__host__ __device__ __forceinline__ unsigned bucket_checksum(int64_t lo, int64_t size) {
+    const uint64_t a = (uint64_t)lo + 1, b = (uint64_t)(lo + size);  // first and last index + 1
+    return (unsigned)(((a + b) * (uint64_t)size) / 2);
 }
 
 // Bucket table for the grouped traversal: the maximal subtrees holding at
 // most `max_size` bodies (a node qualifies when it is small enough and its
 // parent is not).  Such buckets are contiguous in the sorted order and
 // spatially compact (a radix-tree node covers one key prefix).  Appended in
-// any order; ws[0] receives the count, ws[1] (the traversal's work counter)
-// is reset.
+// any order; ws[0] receives the count and ws[3] the table's checksum,
+// ws[1] (the traversal's work counter) is reset.
 __global__ void __launch_bounds__(256) k_make_buckets(const int2 *__restrict__ ranges,
                                                       const int32_t *__restrict__ parents,
                                                       int64_t n, int max_size,
@@ -109,7 +155,94 @@ __global__ void __launch_bounds__(256) k_make_buckets(const int2 *__restrict__ r
         if (top) {
             const int slot = atomicAdd(ws, 1);
             buckets[slot] = make_int4(lo, size, (int)v, 0);
+            atomicAdd(reinterpret_cast<unsigned *>(ws + 3), bucket_checksum(lo, size));
         }
+    }
+}
+
+// Appends this warp's buckets of one table: for every lane's node holding more
+// than max_size bodies, each child holding at most max_size (e0: the left
+// child [lo, gamma], e1: the right child [gamma + 1, hi]), and the root when
+// the whole tree fits (er).  One atomic per warp; every lane of the warp calls.
+__device__ __forceinline__ void append_buckets(int32_t *ws, bool e0, bool e1, bool er, int lo,
+                                               int gamma, int hi, int32_t c0, int32_t c1,
+                                               int32_t root) {
+    const unsigned b0 = __ballot_sync(0xffffffffu, e0), b1 = __ballot_sync(0xffffffffu, e1),
+                   br = __ballot_sync(0xffffffffu, er);
+    const int n0 = __popc(b0), n1 = __popc(b1), total = n0 + n1 + __popc(br);
+    if (total == 0) return;
+    const int lane = threadIdx.x & 31;
+    int base = 0;
+    if (lane == 0) base = atomicAdd(ws, total);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    const unsigned lt = (1u << lane) - 1u;
+    int4 *buckets = reinterpret_cast<int4 *>(ws + 4);
+    unsigned sum = 0;
+    if (e0) {
+        buckets[base + __popc(b0 & lt)] = make_int4(lo, gamma - lo + 1, c0, 0);
+        sum += bucket_checksum(lo, gamma - lo + 1);
+    }
+    if (e1) {
+        buckets[base + n0 + __popc(b1 & lt)] = make_int4(gamma + 1, hi - gamma, c1, 0);
+        sum += bucket_checksum(gamma + 1, hi - gamma);
+    }
+    if (er) {
+        buckets[base + n0 + n1 + __popc(br & lt)] = make_int4(lo, hi - lo + 1, root, 0);
+        sum += bucket_checksum(lo, hi - lo + 1);
+    }
+    sum = __reduce_add_sync(0xffffffffu, sum);
+    if (lane == 0) atomicAdd(reinterpret_cast<unsigned *>(ws + 3), sum);
+}
+
+// The build fused with the bookkeeping of a grouped step: one thread per
+// split i forms internal node n + i exactly as k_build_tree does, records
+// its body range, zeroes its climb counter and appends its bucket children
+// to the bucket table (ws, buckets of at most max_size bodies) and, when
+// sws is given, to the super-bucket table (at most super_size): the same
+// sets k_make_buckets finds, in another order.  The root is always node n
+// (no split has node n as a child), so root_idx is written here and the
+// root's parent, like the leaves' children, keeps the -1 it was given
+// before the first build.  The loop is warp-uniform for the ballots.
+template <typename I>
+__global__ void __launch_bounds__(256) k_build_tree_buckets(
+    const uint64_t *__restrict__ codes, int32_t *__restrict__ children,
+    int32_t *__restrict__ parents, int64_t n, int2 *__restrict__ ranges,
+    int32_t *__restrict__ counters, int32_t *__restrict__ root_idx, int max_size,
+    int32_t *__restrict__ ws, int super_size, int32_t *__restrict__ sws) {
+    const int lane = threadIdx.x & 31;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); base < n - 1;
+         base += stride) {
+        const int64_t i = base + lane;
+        const bool valid = i < n - 1;
+        int64_t lo = 0, hi = 0, gamma = 0;
+        int32_t c0 = -1, c1 = -1;
+        if (valid) {
+            const Split q = split_of<I>(codes, (I)i, (I)n);
+            lo = q.lo;
+            hi = q.hi;
+            gamma = q.gamma;
+            c0 = q.c0;
+            c1 = q.c1;
+            const int64_t idx = i + n;
+            reinterpret_cast<int2 *>(children)[idx] = make_int2(c0, c1);
+            parents[c0] = (int32_t)idx;
+            parents[c1] = (int32_t)idx;
+            ranges[i] = make_int2((int)lo, (int)hi);
+            counters[idx] = 0;
+            if (i == 0 && root_idx) root_idx[0] = (int32_t)n;
+        }
+        const int64_t size = hi - lo + 1, s0 = gamma - lo + 1, s1 = hi - gamma;
+        const int32_t root = (int32_t)n;
+        append_buckets(ws, valid && size > max_size && s0 <= max_size,
+                       valid && size > max_size && s1 <= max_size,
+                       valid && i == 0 && size <= max_size, (int)lo, (int)gamma, (int)hi, c0, c1,
+                       root);
+        if (sws)
+            append_buckets(sws, valid && size > super_size && s0 <= super_size,
+                           valid && size > super_size && s1 <= super_size,
+                           valid && i == 0 && size <= super_size, (int)lo, (int)gamma, (int)hi, c0,
+                           c1, root);
     }
 }
 
@@ -404,7 +537,7 @@ static int make_buckets(const int32_t *ranges, const int32_t *parents, const uin
     int4 *buckets = reinterpret_cast<int4 *>(workspace + 4);
     if (n == 0) return CNB_OK;
     if (n == 1) {
-        const int32_t one[4] = {1, 0, 0, 0};
+        const int32_t one[4] = {1, 0, 0, 1};  // one bucket; checksum 1
         const int32_t b[4] = {0, 1, 0, 0};
         CNB_CUDA(cudaMemcpyAsync(workspace, one, sizeof(one), cudaMemcpyHostToDevice, st));
         CNB_CUDA(cudaMemcpyAsync(buckets, b, sizeof(b), cudaMemcpyHostToDevice, st));
@@ -427,6 +560,38 @@ extern "C" int cnb_make_buckets_boxes(const int32_t *ranges, const int32_t *pare
     if (!codes || box_bits < 0 || box_bits > 30) return CNB_E_INVALID_ARG;
     return make_buckets(ranges, parents, codes, 3 * ((63 - box_bits) / 3), n, max_size,
                         workspace, stream);
+}
+
+extern "C" int cnb_build_tree_buckets(const uint64_t *codes, int32_t *children, int32_t *parents,
+                                      int32_t *ranges, int32_t *counters, int32_t *root_idx,
+                                      int64_t n, int max_size, int32_t *workspace, int super_size,
+                                      int32_t *super_ws, void *stream) {
+    if (n < 0 || max_size < 1 || !workspace || !root_idx) return CNB_E_INVALID_ARG;
+    if (super_ws && super_size < 1) return CNB_E_INVALID_ARG;
+    if (n > 1 && (!codes || !children || !parents || !ranges || !counters)) return CNB_E_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(ranges) & 7) || (reinterpret_cast<uintptr_t>(children) & 7) ||
+        (reinterpret_cast<uintptr_t>(workspace) & 15) || (reinterpret_cast<uintptr_t>(super_ws) & 15))
+        return CNB_E_INVALID_ARG;
+    if (2 * n - 1 > (int64_t)INT32_MAX) return CNB_E_TOO_LARGE;
+    cudaStream_t st = as_stream(stream);
+    if (n < 2) {
+        // one body (or none): the root is leaf 0 and the only bucket
+        CNB_CUDA(cudaMemsetAsync(root_idx, 0, 4, st));
+        CNB_TRY(make_buckets(ranges, parents, nullptr, 0, n, max_size, workspace, stream));
+        if (super_ws) CNB_TRY(make_buckets(ranges, parents, nullptr, 0, n, super_size, super_ws, stream));
+        return CNB_OK;
+    }
+    CNB_CUDA(cudaMemsetAsync(workspace, 0, 16, st));
+    if (super_ws) CNB_CUDA(cudaMemsetAsync(super_ws, 0, 16, st));
+    if (n <= (int64_t)1 << 29)
+        k_build_tree_buckets<int><<<grid_for(n - 1, 256), 256, 0, st>>>(
+            codes, children, parents, n, reinterpret_cast<int2 *>(ranges), counters, root_idx,
+            max_size, workspace, super_ws ? super_size : 0, super_ws);
+    else
+        k_build_tree_buckets<int64_t><<<grid_for(n - 1, 256), 256, 0, st>>>(
+            codes, children, parents, n, reinterpret_cast<int2 *>(ranges), counters, root_idx,
+            max_size, workspace, super_ws ? super_size : 0, super_ws);
+    return launch_status();
 }
 
 static int upward_impl(const float *px, const float *py, const float *pz, const float *mass,

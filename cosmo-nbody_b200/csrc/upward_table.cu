@@ -59,47 +59,74 @@ __device__ __forceinline__ float3 centre_of(float4 s) {
     return make_float3(__fmul_rn(s.x, inv), __fmul_rn(s.y, inv), __fmul_rn(s.z, inv));
 }
 
+// The parent of children L and R: tree_kernels.py:174-188 (left + right),
+// min, max, and (QUAD) the second central moment from the children's
+// moments and centres, left child first, then right.
+template <bool QUAD>
+__device__ __forceinline__ void combine(float4 Ls, float4 Llo, float4 Lhi, float4 La, float4 Lb,
+                                        float4 Rs, float4 Rlo, float4 Rhi, float4 Ra, float4 Rb,
+                                        float4 &qs, float4 &qlo, float4 &qhi, float4 &na,
+                                        float4 &nb) {
+    qs = make_float4(__fadd_rn(Ls.x, Rs.x), __fadd_rn(Ls.y, Rs.y), __fadd_rn(Ls.z, Rs.z),
+                     __fadd_rn(Ls.w, Rs.w));
+    qlo = make_float4(umin(Llo.x, Rlo.x), umin(Llo.y, Rlo.y), umin(Llo.z, Rlo.z), 0.f);
+    qhi = make_float4(umax(Lhi.x, Rhi.x), umax(Lhi.y, Rhi.y), umax(Lhi.z, Rhi.z), 0.f);
+    if (QUAD) {
+        const float3 cp = centre_of(qs), cl = centre_of(Ls), cr = centre_of(Rs);
+        na = make_float4(__fadd_rn(La.x, Ra.x), __fadd_rn(La.y, Ra.y), __fadd_rn(La.z, Ra.z),
+                         __fadd_rn(La.w, Ra.w));
+        nb = make_float4(__fadd_rn(Lb.x, Rb.x), __fadd_rn(Lb.y, Rb.y), 0.f, 0.f);
+        moment_add(na, nb, Ls.w, __fsub_rn(cl.x, cp.x), __fsub_rn(cl.y, cp.y), __fsub_rn(cl.z, cp.z));
+        moment_add(na, nb, Rs.w, __fsub_rn(cr.x, cp.x), __fsub_rn(cr.y, cp.y), __fsub_rn(cr.z, cp.z));
+    }
+}
+
+// Writes internal node p: its traversal record and box, its raw sums when
+// keep_sums (read again only by climbs) and (QUAD) its moment, with b_max in
+// the record's 3-D-extent slot.
+template <bool QUAD>
+__device__ __forceinline__ void write_node(int64_t p, float4 qs, float4 qlo, float4 qhi,
+                                           float4 na, float4 nb, int2 ch, float4 *sums,
+                                           float4 *rec, float4 *aabb, float4 *quad,
+                                           bool keep_sums) {
+    if (keep_sums) sums[p] = qs;
+    const float sx = qhi.x - qlo.x;
+    float ext = fmaxf(sx, fmaxf(qhi.y - qlo.y, qhi.z - qlo.z));
+    if (QUAD) {
+        quad[2 * p] = na;
+        quad[2 * p + 1] = nb;
+        const float3 cp = centre_of(qs);
+        const float bx = fmaxf(__fsub_rn(cp.x, qlo.x), __fsub_rn(qhi.x, cp.x));
+        const float by = fmaxf(__fsub_rn(cp.y, qlo.y), __fsub_rn(qhi.y, cp.y));
+        const float bz = fmaxf(__fsub_rn(cp.z, qlo.z), __fsub_rn(qhi.z, cp.z));
+        ext = __fsqrt_rn(__fmaf_rn(bx, bx, __fmaf_rn(by, by, __fmul_rn(bz, bz))));
+    }
+    rec[2 * p] = normalised(qs);
+    rec[2 * p + 1] = make_float4(sx, ext, __int_as_float(ch.x), __int_as_float(ch.y));
+    aabb[2 * p] = qlo;
+    aabb[2 * p + 1] = qhi;
+}
+
 // Forms parent p from this node (s, lo, hi, moment qa/qb) and its sibling
-// (bs, blo, bhi, ba/bb): tree_kernels.py:174-188 (left + right), min, max;
-// writes the sums, the traversal record and (QUAD) the moment and b_max, and
-// leaves the parent's values in s, lo, hi, qa, qb.
+// (bs, blo, bhi, ba/bb), writes it, and leaves the parent's values in s, lo,
+// hi, qa, qb.
 template <bool QUAD>
 __device__ __forceinline__ void form_node(int64_t p, int2 ch, bool mine_left, float4 &s,
                                           float4 &lo, float4 &hi, float4 &qa, float4 &qb,
                                           float4 bs, float4 blo, float4 bhi, float4 ba,
                                           float4 bb, float4 *sums, float4 *rec, float4 *aabb,
                                           float4 *quad, bool keep_sums = true) {
-    const float4 &Ls = mine_left ? s : bs, &Rs = mine_left ? bs : s;
-    const float4 &Llo = mine_left ? lo : blo, &Rlo = mine_left ? blo : lo;
-    const float4 &Lhi = mine_left ? hi : bhi, &Rhi = mine_left ? bhi : hi;
-    const float4 qs = make_float4(__fadd_rn(Ls.x, Rs.x), __fadd_rn(Ls.y, Rs.y),
-                                  __fadd_rn(Ls.z, Rs.z), __fadd_rn(Ls.w, Rs.w));
-    const float4 qlo = make_float4(umin(Llo.x, Rlo.x), umin(Llo.y, Rlo.y), umin(Llo.z, Rlo.z), 0.f);
-    const float4 qhi = make_float4(umax(Lhi.x, Rhi.x), umax(Lhi.y, Rhi.y), umax(Lhi.z, Rhi.z), 0.f);
-    if (keep_sums) sums[p] = qs;  // the raw sums are read again only by climbs
-    store_record(rec, aabb, p, qs, qlo, qhi, ch.x, ch.y);
-    if (QUAD) {
-        // left child first, then right: the same bits whichever child arrives second
-        const float4 &La = mine_left ? qa : ba, &Ra = mine_left ? ba : qa;
-        const float4 &Lb = mine_left ? qb : bb, &Rb = mine_left ? bb : qb;
-        const float3 cp = centre_of(qs), cl = centre_of(Ls), cr = centre_of(Rs);
-        float4 na = make_float4(__fadd_rn(La.x, Ra.x), __fadd_rn(La.y, Ra.y), __fadd_rn(La.z, Ra.z),
-                                __fadd_rn(La.w, Ra.w));
-        float4 nb = make_float4(__fadd_rn(Lb.x, Rb.x), __fadd_rn(Lb.y, Rb.y), 0.f, 0.f);
-        moment_add(na, nb, Ls.w, __fsub_rn(cl.x, cp.x), __fsub_rn(cl.y, cp.y), __fsub_rn(cl.z, cp.z));
-        moment_add(na, nb, Rs.w, __fsub_rn(cr.x, cp.x), __fsub_rn(cr.y, cp.y), __fsub_rn(cr.z, cp.z));
-        quad[2 * p] = na;
-        quad[2 * p + 1] = nb;
-        const float bx = fmaxf(__fsub_rn(cp.x, qlo.x), __fsub_rn(qhi.x, cp.x));
-        const float by = fmaxf(__fsub_rn(cp.y, qlo.y), __fsub_rn(qhi.y, cp.y));
-        const float bz = fmaxf(__fsub_rn(cp.z, qlo.z), __fsub_rn(qhi.z, cp.z));
-        rec[2 * p + 1].y = __fsqrt_rn(__fmaf_rn(bx, bx, __fmaf_rn(by, by, __fmul_rn(bz, bz))));
-        qa = na;
-        qb = nb;
-    }
+    float4 qs, qlo, qhi, na = qa, nb = qb;
+    if (mine_left)
+        combine<QUAD>(s, lo, hi, qa, qb, bs, blo, bhi, ba, bb, qs, qlo, qhi, na, nb);
+    else
+        combine<QUAD>(bs, blo, bhi, ba, bb, s, lo, hi, qa, qb, qs, qlo, qhi, na, nb);
+    write_node<QUAD>(p, qs, qlo, qhi, na, nb, ch, sums, rec, aabb, quad, keep_sums);
     s = qs;
     lo = qlo;
     hi = qhi;
+    qa = na;
+    qb = nb;
 }
 
 // One node's climb towards the root with the global atomic counters: the
@@ -117,7 +144,11 @@ __device__ __forceinline__ void climb(int64_t curr, float4 s, float4 lo, float4 
             set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
             break;
         }
-        if (p == -1) break;
+        if (p == -1) {
+            // only the tree's root (node n; leaf 0 for one body) has no parent
+            if (curr != (n > 1 ? n : 0)) set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
+            break;
+        }
         if (p < 0 || p >= m_nodes) {
             set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
             break;
@@ -127,10 +158,16 @@ __device__ __forceinline__ void climb(int64_t curr, float4 s, float4 lo, float4 
         const int2 ch = __ldg(children + p);
         const int32_t pp = __ldg(parents + p);
         // release this node's data, acquire the sibling's: the first arrival stops
-        if (atomic_add_acq_rel(counts + p, 1) == 0) break;
+        // (after the check that p is this node's parent, which every arrival makes)
+        const int32_t arrived = atomic_add_acq_rel(counts + p, 1);
         const bool mine_left = (ch.x == curr);
+        if (!mine_left && ch.y != curr) {
+            set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
+            break;
+        }
+        if (arrived == 0) break;
         const int32_t sib = mine_left ? ch.y : ch.x;
-        if ((!mine_left && ch.y != curr) || sib == curr || sib < 0 || sib >= m_nodes) {
+        if (sib == curr || sib < 0 || sib >= m_nodes) {
             set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
             break;
         }
@@ -174,99 +211,217 @@ __global__ void __launch_bounds__(256) k_upward_table(
 }
 
 // ---------------------------------------------------------------- by buckets
-// The same pass in two phases over the bucket table (maximal subtrees of at
-// most kUpSlots bodies): one warp per bucket forms every node inside its
-// bucket with shared-memory counters and keeps the nodes' data in shared
-// memory, so a level costs a shared-memory atomic instead of an L2 round
-// trip; then one thread per bucket root climbs the levels above with the
-// global counters.  Every node is still formed as (left + right) of its
-// children: the table is bit-identical to the one-phase pass.
+// The same pass over the bucket table (maximal subtrees of at most kUpSlots
+// bodies), one warp per bucket, level by level in shared memory.  A
+// radix-tree subtree over bodies [lo, hi] whose root is node n + lo holds the
+// internal nodes n + lo .. n + hi - 1, one whose root is n + hi holds
+// n + lo + 1 .. n + hi (the left child of a node is named by its last body,
+// the right child by its first), so the bucket's children are one coalesced
+// read.  The warp checks that they form a tree over the bucket's bodies
+// (every body and node but the root has exactly one parent), loads the
+// leaves, and then forms, round after round, every node whose two children
+// are ready; each lane owns at most two of the bucket's nodes, no lane waits
+// on another and no atomic is needed.  Every node is formed as
+// (left + right) of its children: the table is bit-identical to the
+// one-phase pass.  CLIMB: after every 32 buckets a warp climbs on above
+// their roots, one lane each, with the global counters (the first arrival at
+// a node stops, as in the one-phase pass); otherwise k_upward_roots does that
+// in a second launch.
 constexpr int kUpSlots = 64;  // leaves of a bucket; its internal nodes use as many slots
 constexpr int kUpWarps = 4;
 
+// Climbs above the bucket roots one lane each (root < 0: nothing), reading a
+// root's sums and box back from global memory; the roots were formed by
+// other lanes of this warp, whose writes the fence and the warp barrier
+// order before this lane's release at the first counter.
 template <bool QUAD>
+__device__ __forceinline__ void climb_roots(int64_t root, const int2 *__restrict__ children,
+                                            const int32_t *__restrict__ parents, int32_t *counts,
+                                            float4 *sums, float4 *rec, float4 *aabb, float4 *quad,
+                                            int64_t n, int32_t *status) {
+    __threadfence();
+    __syncwarp();
+    if (root >= 0) {
+        const float4 s = __ldcg(sums + root);
+        const float4 lo = __ldcg(aabb + 2 * root), hi = __ldcg(aabb + 2 * root + 1);
+        float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;
+        if (QUAD && root >= n) {
+            qa = __ldcg(quad + 2 * root);
+            qb = __ldcg(quad + 2 * root + 1);
+        }
+        climb<QUAD>(root, s, lo, hi, qa, qb, children, parents, counts, sums, rec, aabb, quad, n,
+                    status);
+    }
+    __syncwarp();
+}
+
+template <bool QUAD, bool CLIMB>
 __global__ void __launch_bounds__(kUpWarps * 32) k_upward_buckets(
     const float *__restrict__ px, const float *__restrict__ py, const float *__restrict__ pz,
     const float *__restrict__ mass, const int2 *__restrict__ children,
-    const int32_t *__restrict__ parents, const int32_t *__restrict__ ws, float4 *sums,
-    float4 *rec, float4 *aabb, float4 *quad, int64_t n, int32_t *status) {
+    const int32_t *__restrict__ parents, const int32_t *__restrict__ ws, int32_t *counts,
+    float4 *sums, float4 *rec, float4 *aabb, float4 *quad, int64_t n, int32_t *status) {
     // slot k < kUpSlots: leaf lo + k; slot kUpSlots + k: internal node n + lo + k
     __shared__ float4 s_sum[kUpWarps][2 * kUpSlots], s_lo[kUpWarps][2 * kUpSlots],
         s_hi[kUpWarps][2 * kUpSlots];
     __shared__ float4 s_qa[QUAD ? kUpWarps : 1][QUAD ? 2 * kUpSlots : 1],
         s_qb[QUAD ? kUpWarps : 1][QUAD ? 2 * kUpSlots : 1];
-    __shared__ int s_cnt[kUpWarps][kUpSlots];
+    __shared__ int s_par[kUpWarps][2 * kUpSlots];  // parent (internal index) of each slot
+    __shared__ int s_rdy[kUpWarps][2 * kUpSlots];  // the slot's data is in shared memory
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int nb = ws[0];
     const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
-    for (int g = blockIdx.x * kUpWarps + w; g < nb; g += gridDim.x * kUpWarps) {
-        const int4 bk = buckets[g];
+    // the buckets tile the bodies once (the table's checksum, see bucket_checksum)
+    if (blockIdx.x == 0 && threadIdx.x == 0 &&
+        (unsigned)ws[3] != (unsigned)((uint64_t)n * (uint64_t)(n + 1) / 2))
+        set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
+    int64_t my_root = -1;  // CLIMB: the bucket root this lane climbs from
+    const int stride = gridDim.x * kUpWarps;
+    int4 bk_next = make_int4(0, 0, 0, 0);
+    if (blockIdx.x * kUpWarps + w < nb) bk_next = buckets[blockIdx.x * kUpWarps + w];
+    for (int g = blockIdx.x * kUpWarps + w, t = 0; g < nb; g += stride, ++t) {
+        if (CLIMB && t > 0 && (t & 31) == 0) {
+            climb_roots<QUAD>(my_root, children, parents, counts, sums, rec, aabb, quad, n, status);
+            my_root = -1;
+        }
+        const int4 bk = bk_next;
+        if (g + stride < nb) bk_next = buckets[g + stride];  // in flight during this bucket
         const int lo_b = bk.x, count = bk.y;
         const int64_t root = bk.z;
-        if (count < 1 || count > kUpSlots) {
+        const int off = (count > 1 && root == n + lo_b + count - 1) ? 1 : 0;  // first internal slot
+        const int root_slot = count == 1 ? 0 : kUpSlots + (int)(root - n - lo_b);
+        if (count > kUpSlots) {
             if (lane == 0) set_flag(status, CNB_FLAG_LIST_OVERFLOW);
             continue;
         }
-        for (int k = lane; k < kUpSlots; k += 32) s_cnt[w][k] = 0;
-        __syncwarp();
-        for (int k = lane; k < count; k += 32) {
-            const int64_t i = lo_b + k;
-            const float m = mass[i], x = px[i], y = py[i], z = pz[i];
-            float4 s = make_float4(__fmul_rn(x, m), __fmul_rn(y, m), __fmul_rn(z, m), m);
-            float4 lo = make_float4(x, y, z, 0.f), hi = lo;
-            float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;
-            // raw sums go to global memory only for the bucket root (phase two reads them)
-            if (i == root) sums[i] = s;
-            store_record(rec, aabb, i, s, lo, hi, -1, -1);
-            s_sum[w][k] = s;
-            s_lo[w][k] = lo;
-            s_hi[w][k] = hi;
-            if (QUAD) {
-                s_qa[w][k] = qa;
-                s_qb[w][k] = qb;
+        if (count < 1 || lo_b < 0 || (int64_t)lo_b + count > n || root >= 2 * n - 1 ||
+            (count == 1 ? root != lo_b : root != n + lo_b && root != n + lo_b + count - 1)) {
+            if (lane == 0) set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
+            continue;
+        }
+        // every global read of the bucket at once: its leaves and its internal nodes' children
+        float4 leaf[2];  // (x, y, z, m) of bodies lo + lane and lo + lane + 32
+        int2 chn[2];
+        bool own[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            leaf[h] = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k < count) {
+                const int64_t i = lo_b + k;
+                leaf[h] = make_float4(px[i], py[i], pz[i], mass[i]);
             }
-            int64_t curr = i;
-            for (int guard = 0; curr != root; ++guard) {
-                const int32_t p = parents[curr];
-                const int64_t ps = (int64_t)p - n - lo_b;
-                if (guard > 2 * kUpSlots || ps < 0 || ps >= count) {
-                    set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
-                    break;
-                }
-                const int2 ch = __ldg(children + p);
-                __threadfence_block();  // this node's data before the count
-                if (atomicAdd(&s_cnt[w][ps], 1) == 0) break;
-                __threadfence_block();  // the sibling's data after the count
-                const bool mine_left = (ch.x == curr);
-                const int32_t sib = mine_left ? ch.y : ch.x;
-                const int64_t so = sib < n ? (int64_t)sib - lo_b : kUpSlots + (int64_t)sib - n - lo_b;
-                const int64_t lim = sib < n ? count : kUpSlots + count;
-                if ((!mine_left && ch.y != curr) || sib == curr || sib < 0 ||
-                    so < (sib < n ? 0 : kUpSlots) || so >= lim) {
-                    set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
-                    break;
-                }
-                const float4 bs = s_sum[w][so], blo = s_lo[w][so], bhi = s_hi[w][so];
-                float4 ba = make_float4(0.f, 0.f, 0.f, 0.f), bb = ba;
-                if (QUAD) {
-                    ba = s_qa[w][so];
-                    bb = s_qb[w][so];
-                }
-                form_node<QUAD>(p, ch, mine_left, s, lo, hi, qa, qb, bs, blo, bhi, ba, bb, sums, rec,
-                                aabb, quad, p == root);
-                const int ns = kUpSlots + (int)ps;
-                s_sum[w][ns] = s;
-                s_lo[w][ns] = lo;
-                s_hi[w][ns] = hi;
-                if (QUAD) {
-                    s_qa[w][ns] = qa;
-                    s_qb[w][ns] = qb;
-                }
-                curr = p;
-            }
+            own[h] = off + k < off + count - 1;
+            chn[h] = own[h] ? __ldg(children + n + lo_b + off + k) : make_int2(-1, -1);
+        }
+        for (int k = lane; k < 2 * kUpSlots; k += 32) {
+            s_par[w][k] = -1;
+            s_rdy[w][k] = k < count;  // the leaves are ready once stored
         }
         __syncwarp();
+        // this lane's internal nodes: slots kUpSlots + off + lane (+ 32), children at a[][]
+        int a[2][2];
+        bool bad = false;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = off + lane + 32 * h;
+            a[h][0] = a[h][1] = 0;
+            if (!own[h]) continue;
+            bool ok = true;
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+                const int64_t v = c == 0 ? chn[h].x : chn[h].y;
+                const int64_t r = v < n ? v - lo_b : v - n - lo_b;
+                ok = ok && v >= 0 && (v < n ? r >= 0 && r < count : r >= off && r < off + count - 1);
+                a[h][c] = ok ? (v < n ? (int)r : kUpSlots + (int)r) : 0;
+            }
+            if (ok && a[h][0] != a[h][1])
+                bad |= (atomicExch(&s_par[w][a[h][0]], k) != -1) |
+                       (atomicExch(&s_par[w][a[h][1]], k) != -1);
+            else
+                bad = true;
+        }
+        __syncwarp();
+        // a tree: every slot but the root has exactly one parent, the root none
+        for (int k = lane; k < count; k += 32) bad |= (s_par[w][k] < 0) != (k == root_slot);
+        for (int k = off + lane; k < off + count - 1; k += 32)
+            bad |= (s_par[w][kUpSlots + k] < 0) != (kUpSlots + k == root_slot);
+        if (__any_sync(0xffffffffu, bad)) {
+            if (lane == 0) set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
+            continue;
+        }
+        // the leaves
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = lane + 32 * h;
+            if (k >= count) continue;
+            const int64_t i = lo_b + k;
+            const float x = leaf[h].x, y = leaf[h].y, z = leaf[h].z, m = leaf[h].w;
+            const float4 sv = make_float4(__fmul_rn(x, m), __fmul_rn(y, m), __fmul_rn(z, m), m);
+            const float4 lv = make_float4(x, y, z, 0.f);
+            // raw sums go to global memory only for the bucket root (the climb above reads them)
+            if (i == root) sums[i] = sv;
+            store_record(rec, aabb, i, sv, lv, lv, -1, -1);
+            s_sum[w][k] = sv;
+            s_lo[w][k] = lv;
+            s_hi[w][k] = lv;
+            if (QUAD) s_qa[w][k] = s_qb[w][k] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        __syncwarp();
+        // the internal nodes, round by round (a round forms every node whose
+        // children are ready; a valid bucket needs at most count - 1 rounds)
+        bool done[2] = {!own[0], !own[1]};
+        for (int round = 0; round < count; ++round) {
+            bool formed[2] = {false, false};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                if (done[h] || !s_rdy[w][a[h][0]] || !s_rdy[w][a[h][1]]) continue;
+                const int l = a[h][0], r = a[h][1], ns = kUpSlots + off + lane + 32 * h;
+                const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+                float4 qs, qlo, qhi, na = zero, nb = zero;
+                combine<QUAD>(s_sum[w][l], s_lo[w][l], s_hi[w][l], QUAD ? s_qa[w][l] : zero,
+                              QUAD ? s_qb[w][l] : zero, s_sum[w][r], s_lo[w][r], s_hi[w][r],
+                              QUAD ? s_qa[w][r] : zero, QUAD ? s_qb[w][r] : zero, qs, qlo, qhi, na,
+                              nb);
+                s_sum[w][ns] = qs;
+                s_lo[w][ns] = qlo;
+                s_hi[w][ns] = qhi;
+                if (QUAD) {
+                    s_qa[w][ns] = na;
+                    s_qb[w][ns] = nb;
+                }
+                formed[h] = true;
+            }
+            __syncwarp();  // the data of this round's nodes before their flags
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (formed[h]) {
+                    s_rdy[w][kUpSlots + off + lane + 32 * h] = 1;
+                    done[h] = true;
+                }
+            __syncwarp();
+            if (!__any_sync(0xffffffffu, !(done[0] && done[1]))) break;
+        }
+        // a cycle among the internal nodes leaves some of them unformed
+        if (__any_sync(0xffffffffu, !(done[0] && done[1]))) {
+            if (lane == 0) set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
+            continue;
+        }
+        // the records of the bucket's internal nodes, consecutive nodes on consecutive lanes
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!own[h]) continue;
+            const int k = off + lane + 32 * h, ns = kUpSlots + k;
+            const int64_t p = n + lo_b + k;
+            write_node<QUAD>(p, s_sum[w][ns], s_lo[w][ns], s_hi[w][ns],
+                             QUAD ? s_qa[w][ns] : make_float4(0.f, 0.f, 0.f, 0.f),
+                             QUAD ? s_qb[w][ns] : make_float4(0.f, 0.f, 0.f, 0.f), chn[h], sums,
+                             rec, aabb, quad, p == root);
+        }
+        if (CLIMB && lane == (t & 31)) my_root = root;
     }
+    if (CLIMB)
+        climb_roots<QUAD>(my_root, children, parents, counts, sums, rec, aabb, quad, n, status);
 }
 
 // Phase two: from every bucket root to the tree's root.
@@ -362,6 +517,31 @@ extern "C" int cnb_upward_table_quad(const float *px, const float *py, const flo
     return launch_status();
 }
 
+#ifndef CNB_UPWARD_CLIMB
+#define CNB_UPWARD_CLIMB 1
+#endif
+
+template <bool QUAD>
+static int launch_upward_buckets(const float *px, const float *py, const float *pz,
+                                 const float *mass, const int2 *ch, const int32_t *parents,
+                                 const int32_t *workspace, int32_t *counts, float4 *sums,
+                                 float4 *rec, float4 *aabb, float4 *quad, int64_t n,
+                                 int32_t *status, cudaStream_t st) {
+    constexpr bool kMode = CNB_UPWARD_CLIMB != 0;
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_upward_buckets<QUAD, kMode>,
+                                                  kUpWarps * 32, 0);
+    k_upward_buckets<QUAD, kMode><<<kSMs * (per_sm > 0 ? per_sm : 1), kUpWarps * 32, 0, st>>>(
+        px, py, pz, mass, ch, parents, workspace, counts, sums, rec, aabb, quad, n, status);
+    CNB_TRY(launch_status());
+    if (!kMode) {
+        k_upward_roots<QUAD><<<kSMs * 4, 128, 0, st>>>(ch, parents, workspace, counts, sums, rec,
+                                                       aabb, quad, n, status);
+        CNB_TRY(launch_status());
+    }
+    return CNB_OK;
+}
+
 extern "C" int cnb_upward_table_buckets(const float *px, const float *py, const float *pz,
                                         const float *mass, const int32_t *children,
                                         const int32_t *parents, const int32_t *workspace,
@@ -384,20 +564,10 @@ extern "C" int cnb_upward_table_buckets(const float *px, const float *py, const 
     float4 *s4 = reinterpret_cast<float4 *>(sums);
     cudaStream_t st = as_stream(stream);
     // the bucket count is on the device: persistent grids over the buckets
-    if (quad)
-        k_upward_buckets<true><<<kSMs * 8, kUpWarps * 32, 0, st>>>(
-            px, py, pz, mass, ch, parents, workspace, s4, rec, rec + 2 * m, q4, n, status);
-    else
-        k_upward_buckets<false><<<kSMs * 8, kUpWarps * 32, 0, st>>>(
-            px, py, pz, mass, ch, parents, workspace, s4, rec, rec + 2 * m, nullptr, n, status);
-    CNB_TRY(launch_status());
-    if (quad)
-        k_upward_roots<true><<<kSMs * 4, 128, 0, st>>>(ch, parents, workspace, counts, s4, rec,
-                                                       rec + 2 * m, q4, n, status);
-    else
-        k_upward_roots<false><<<kSMs * 4, 128, 0, st>>>(ch, parents, workspace, counts, s4, rec,
-                                                        rec + 2 * m, nullptr, n, status);
-    return launch_status();
+    if (quad) return launch_upward_buckets<true>(px, py, pz, mass, ch, parents, workspace, counts,
+                                                 s4, rec, rec + 2 * m, q4, n, status, st);
+    return launch_upward_buckets<false>(px, py, pz, mass, ch, parents, workspace, counts, s4, rec,
+                                        rec + 2 * m, nullptr, n, status, st);
 }
 
 extern "C" int cnb_unpack_nodes(const float *node_table, float *n_mass, float *n_com,

@@ -258,10 +258,28 @@ int cnb_build_tree_ranges(const uint64_t *codes, int32_t *children, int32_t *par
 /* Bucket table for cnb_forces_grouped (no reference counterpart): the
  * maximal subtrees holding at most max_size bodies.  workspace (device,
  * 16-byte aligned) is int32 [4 + 4N]: [0] bucket count, [1] work counter,
- * [2] deepest node stack seen by the traversal, [3] unused, then one
+ * [2] deepest node stack seen by the traversal, [3] the bodies' (index + 1)
+ * summed over all buckets modulo 2^32 (N(N+1)/2 when the buckets tile the
+ * bodies once; cnb_upward_table_buckets flags CNB_FLAG_BAD_TOPOLOGY
+ * otherwise, and also when a bucket's nodes do not form a tree over its
+ * bodies: the reference's tie rule for equal keys can leave a node without a
+ * parent), then one
  * (first body, count, subtree node, 0) record per bucket. */
 int cnb_make_buckets(const int32_t *ranges, const int32_t *parents, int64_t n, int max_size,
                      int32_t *workspace, void *stream);
+
+/* cnb_build_tree_ranges, cnb_make_buckets (max_size) and cnb_find_root in
+ * one launch, for the grouped step: also zeroes the internal nodes' climb
+ * counters (counters int32 [2N-1]) and, when super_ws is not NULL, makes the
+ * super-bucket table of cnb_forces_two_level (super_size bodies) there.  The
+ * root is always node N (leaf 0 for N = 1).  Writes no leaf's children and
+ * not the root's parent: those must hold -1 from an earlier
+ * cnb_reset_tree_buffers (or the allocation).  Bucket tables list the same
+ * buckets as cnb_make_buckets, in another order. */
+int cnb_build_tree_buckets(const uint64_t *codes, int32_t *children, int32_t *parents,
+                           int32_t *ranges, int32_t *counters, int32_t *root_idx, int64_t n,
+                           int max_size, int32_t *workspace, int super_size, int32_t *super_ws,
+                           void *stream);
 
 /* cnb_make_buckets for several boxes in one tree (keys of
  * cnb_compute_codes_boxes): no bucket spans two boxes. */
@@ -311,8 +329,10 @@ int cnb_forces_grouped(const float *px, const float *py, const float *pz,
  * one warp per super-bucket walks the top of the tree once and keeps the
  * nodes every bucket inside it accepts (applied by each bucket from that
  * list) and the nodes only a bucket can decide (each bucket's walk starts
- * there).  ranges / parents: cnb_build_tree_ranges; workspace: the bucket
- * table of cnb_make_buckets; super_ws: device scratch of super_ws_bytes
+ * there).  ranges / parents: cnb_build_tree_ranges, from which the
+ * super-bucket table is made in super_ws; both NULL: super_ws already holds
+ * it (cnb_build_tree_buckets with the same super_bodies); workspace: the
+ * bucket table of cnb_make_buckets; super_ws: device scratch of super_ws_bytes
  * (16-byte aligned), cnb_two_level_workspace_bytes recommends a size; a
  * super-bucket whose lists do not fit there walks from the root. */
 int64_t cnb_two_level_workspace_bytes(int64_t n, int super_bodies);

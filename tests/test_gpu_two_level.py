@@ -247,3 +247,44 @@ def test_engine_two_level_matches_single_level():
         eng.check()
         forces.append(st.force.cpu().numpy())
     _close(forces[1], forces[0])
+
+
+def test_super_size_change_between_builds():
+    """The tree build makes the super-bucket table for the engine's current
+    super-bucket size; after a change of size (as the autotuner makes) the
+    next force call, before any rebuild, makes the table itself and gives the
+    same forces as the single-level walk."""
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils import config as cfgmod
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = cfgmod.make(N_GRID=24, SOFTENING=0.5 / 24, THETA=0.5, N_STEPS=100, A_START=0.02,
+                      A_END=0.22, KEY_MODE="morton63", FORCE_MODE="grouped", BODIES_PER_LANE=2,
+                      BLOCK_WARPS=4, SUPER_BODIES=512)
+    pos, vel = zeldovich_arrays(24, 3)
+    st = SimulationState(24 ** 3, pos, vel)
+    eng = SimulationEngine(cfg, st, camera=False)
+    eng.forces_only()
+    eng.check()
+    tm = eng.tree_manager
+    assert tm.super_table_current
+    f512 = st.force.clone()
+    eng.set_super_bodies(1024)
+    assert not tm.super_table_current
+    st.force.zero_()
+    eng.compute_forces()
+    eng.check()
+    f1024 = st.force.clone()
+    eng.set_super_bodies(0)
+    st.force.zero_()
+    eng.compute_forces()
+    eng.check()
+    f0 = st.force.cpu().numpy()
+    _close(f512.cpu().numpy(), f0)
+    _close(f1024.cpu().numpy(), f0)
+    # the next build makes the 1024-body table again
+    eng.set_super_bodies(1024)
+    eng.forces_only()
+    eng.check()
+    assert tm.super_table_current
+    _close(st.force.cpu().numpy(), f0)
