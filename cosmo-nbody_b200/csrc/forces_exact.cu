@@ -48,21 +48,30 @@
 
 namespace cnb {
 
-constexpr int kXPStack = 256;           // (node, mask) entries per warp for part of a bucket
 constexpr float kCutLo = 0.99999e-7f, kCutHi = 1.00001e-7f;  // float64 band around the cut
 
-// per-warp shared memory: three lists of kGList entries (whole bucket, masked
-// with one image, anything else) and the per-body items of one round
+// The two node stacks of a warp share one region of kXWords words: entries
+// reached by the whole bucket (one word, the node) grow up from word 0,
+// entries reached by part of it (three words: node, mask low, mask high)
+// grow down from the end; a push that would make them meet drops the
+// children and flags CNB_FLAG_LIST_OVERFLOW.  The deepest use measured on
+// 128^3 and 256^3 Zel'dovich and evolved states (two-level walk included) is
+// 568 words; 864 is the most that keeps ten 2-warp blocks (20 warps) per SM.
+constexpr int kXWords = 864;
+__device__ __forceinline__ int part_word(int k) { return kXWords - 3 * (k + 1); }
+
+// per-warp shared memory: the whole-bucket and masked lists (packed for two
+// bodies per lane), the per-pair list (one float4 per entry), the per-body
+// items of one round, the two lists' masks and the stack region
 template <int BPL> __host__ __device__ constexpr int exact_f4_per_warp() {
-    return 3 * kGList * entry_width<BPL>() + 3 * 32;
+    return 2 * kGList * entry_width<BPL>() + kGList + 3 * 32;
 }
-constexpr int kExactMasksPerWarp = 2 * kGList + kXPStack;  // uint2
-constexpr int kExactIntsPerWarp = kGStack + kXPStack;       // int32
+constexpr int kExactMasksPerWarp = 2 * kGList;  // uint2
 
 template <int BPL>
 constexpr size_t exact_smem(int warps) {
     return (size_t)warps * (exact_f4_per_warp<BPL>() * sizeof(float4) +
-                            kExactMasksPerWarp * sizeof(uint2) + kExactIntsPerWarp * sizeof(int32_t));
+                            kExactMasksPerWarp * sizeof(uint2) + kXWords * sizeof(int32_t));
 }
 
 // per-body item flags
@@ -96,11 +105,26 @@ __device__ __forceinline__ bool ref_outside_cut(float dx, float dy, float dz, fl
     return d2d > 1e-7;
 }
 
-// Masked list: cnt entries (two float4 per entry for two bodies per lane, as
-// put_entry writes them) applied to the lane's bodies in the entry's mask.
-// WRAP_CUT: raw CoM with the per-pair minimum image and the cut; otherwise
-// the CoM at the one image every body of the bucket sees, out of the cut's
-// reach.
+// Entry j of a list as the two packed float4 (x, x, y, y), (z, z, m, m) of the
+// two-bodies-per-lane loop: stored so (put_entry), or SINGLE: stored once as
+// (x, y, z, m) and duplicated here (the rarely filled per-pair list).
+template <bool SINGLE>
+__device__ __forceinline__ void entry_pair(const float4 *list, int j, float4 &a, float4 &b) {
+    if (SINGLE) {
+        const float4 e = list[j];
+        a = make_float4(e.x, e.x, e.y, e.y);
+        b = make_float4(e.z, e.z, e.w, e.w);
+    } else {
+        a = list[2 * j];
+        b = list[2 * j + 1];
+    }
+}
+
+// Masked list: cnt entries applied to the lane's bodies in the entry's mask.
+// WRAP_CUT: raw CoM, one float4 per entry, with the per-pair minimum image
+// and the cut; otherwise the CoM at the one image every body of the bucket
+// sees, out of the cut's reach (two float4 per entry for two bodies per
+// lane, as put_entry writes them).
 template <int BPL, bool WRAP_CUT>
 __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *masks, int cnt,
                                              int lane, const float (&x)[BPL], const float (&y)[BPL],
@@ -120,7 +144,8 @@ __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *ma
             float2 dx[8], dy[8], dz[8], w[8], q[8];
 #pragma unroll
             for (int u = 0; u < 8; ++u) {
-                const float4 a = list[2 * (j + u)], b = list[2 * (j + u) + 1];
+                float4 a, b;
+                entry_pair<WRAP_CUT>(list, j + u, a, b);
                 const uint2 mk = masks[j + u];
                 dx[u] = __fadd2_rn(make_float2(a.x, a.y), nx);
                 dy[u] = __fadd2_rn(make_float2(a.z, a.w), ny);
@@ -145,7 +170,8 @@ __device__ __forceinline__ void apply_masked(const float4 *list, const uint2 *ma
             }
         }
         for (; j < cnt; ++j) {
-            const float4 a = list[2 * j], b = list[2 * j + 1];
+            float4 a, b;
+            entry_pair<WRAP_CUT>(list, j, a, b);
             const uint2 mk = masks[j];
             float2 dx = __fadd2_rn(make_float2(a.x, a.y), nx);
             float2 dy = __fadd2_rn(make_float2(a.z, a.w), ny);
@@ -268,7 +294,7 @@ __device__ __forceinline__ void flush32(float4 *lst, uint2 *msk, int &cnt, int l
                                         const float (&x)[BPL], const float (&y)[BPL],
                                         const float (&z)[BPL], float soft2, float (&ax)[BPL],
                                         float (&ay)[BPL], float (&az)[BPL]) {
-    constexpr int EW = entry_width<BPL>();
+    constexpr int EW = KIND == 2 ? 1 : entry_width<BPL>();  // the per-pair list: one float4
     if (KIND == 0) apply_entries<BPL, false, false>(lst, 32, x, y, z, soft2, ax, ay, az);
     else if (KIND == 1) apply_masked<BPL, false>(lst, msk, 32, lane, x, y, z, soft2, ax, ay, az);
     else apply_masked<BPL, true>(lst, msk, 32, lane, x, y, z, soft2, ax, ay, az);
@@ -292,14 +318,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
     float4 *list = f4 + wib * exact_f4_per_warp<BPL>();  // whole bucket, one image, no cut
     float4 *mlist = list + kGList * EW;                   // masked, one image, no cut
     float4 *xlist = mlist + kGList * EW;                  // per-pair image and cut, any mask
-    float4 *plist = xlist + kGList * EW;                  // per-body items (3 float4 each)
+    float4 *plist = xlist + kGList;                       // per-body items (3 float4 each)
     uint2 *mbase = reinterpret_cast<uint2 *>(f4 + WARPS * exact_f4_per_warp<BPL>());
     uint2 *mmask = mbase + wib * kExactMasksPerWarp;
     uint2 *xmask = mmask + kGList;
-    uint2 *psmask = xmask + kGList;
+    // the stack region: whole-bucket entries from word 0 up, (node, mask) entries from the end down
     int32_t *stack = reinterpret_cast<int32_t *>(mbase + WARPS * kExactMasksPerWarp) +
-                     wib * kExactIntsPerWarp;
-    int32_t *pstack = stack + kGStack;
+                     wib * kXWords;
 
     unsigned long long n_tests = 0, n_inter = 0, n_wrap = 0;
     int max_top = 0;
@@ -379,7 +404,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
         if (P.super_of_body) {
             const int sup = P.super_of_body[bk.x];
             const int4 h = sup >= 0 ? P.super_hdr[sup] : make_int4(0, 0, 0, 0);
-            if (h.w) {
+            if (h.w && h.z <= kXWords) {
                 // the nodes every body of the super-bucket accepts (k_super_lists)
                 const float4 *far = P.far_lists + (int64_t)sup * P.far_cap;
                 for (int j0 = 0; j0 < h.x; j0 += 32) {
@@ -423,8 +448,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             int32_t node = -1;
             uint2 mk = fm;
             if (lane < k1) {
-                node = pstack[ptop + lane];
-                mk = psmask[ptop + lane];
+                const int pw = part_word(ptop + lane);
+                node = stack[pw];
+                mk = make_uint2((uint32_t)stack[pw + 1], (uint32_t)stack[pw + 2]);
             } else if (lane < k1 + k2) {
                 node = stack[top + lane - k1];
             }
@@ -491,7 +517,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                     mmask[w] = mk;
                 } else {
                     const int w = xcnt + __popc(m_x & lt);
-                    put_entry<BPL>(xlist, w, A);
+                    xlist[w] = A;
                     xmask[w] = mk;
                     n_wrap += nb;
                 }
@@ -500,7 +526,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             mcnt += __popc(m_msk);
             xcnt += __popc(m_x);
             const int n_ow = __popc(m_ow), n_op = __popc(m_op);
-            if (top + 2 * n_ow > kGStack || ptop + 2 * n_op > kXPStack) {
+            if (top + 2 * n_ow + 3 * (ptop + 2 * n_op) > kXWords) {
                 overflow = true;  // children dropped (flagged)
             } else {
                 if (cls == 2 && whole) {
@@ -510,10 +536,13 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                 }
                 if (cls == 2 && !whole) {
                     const int pos = ptop + 2 * __popc(m_op & lt);
-                    pstack[pos] = c1;
-                    pstack[pos + 1] = c0;
-                    psmask[pos] = mk;
-                    psmask[pos + 1] = mk;
+                    const int w1 = part_word(pos), w0 = part_word(pos + 1);
+                    stack[w1] = c1;
+                    stack[w1 + 1] = (int32_t)mk.x;
+                    stack[w1 + 2] = (int32_t)mk.y;
+                    stack[w0] = c0;
+                    stack[w0 + 1] = (int32_t)mk.x;
+                    stack[w0 + 2] = (int32_t)mk.y;
                 }
                 top += 2 * n_ow;
                 ptop += 2 * n_op;
@@ -561,7 +590,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                 const uint32_t mw = __ballot_sync(0xffffffffu, has && whole_o);
                 const uint32_t mp = __ballot_sync(0xffffffffu, has && !whole_o);
                 const int nw = __popc(mw), npart = __popc(mp);
-                if (top + 2 * nw > kGStack || ptop + 2 * npart > kXPStack) {
+                if (top + 2 * nw + 3 * (ptop + 2 * npart) > kXWords) {
                     overflow = true;  // children dropped (flagged)
                 } else {
                     if (has && whole_o) {
@@ -571,16 +600,19 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                     }
                     if (has && !whole_o) {
                         const int pos = ptop + 2 * __popc(mp & lt);
-                        pstack[pos] = k1c;
-                        pstack[pos + 1] = k0;
-                        psmask[pos] = my_om;
-                        psmask[pos + 1] = my_om;
+                        const int w1 = part_word(pos), w0 = part_word(pos + 1);
+                        stack[w1] = k1c;
+                        stack[w1 + 1] = (int32_t)my_om.x;
+                        stack[w1 + 2] = (int32_t)my_om.y;
+                        stack[w0] = k0;
+                        stack[w0 + 1] = (int32_t)my_om.x;
+                        stack[w0 + 2] = (int32_t)my_om.y;
                     }
                     top += 2 * nw;
                     ptop += 2 * npart;
                 }
             }
-            max_top = max(max_top, top + ptop);
+            max_top = max(max_top, top + 3 * ptop);  // words of the stack region
             __syncwarp();
             if (cnt >= 32) flush32<BPL, 0>(list, nullptr, cnt, lane, x, y, z, soft2, ax, ay, az);
             if (mcnt >= 32) flush32<BPL, 1>(mlist, mmask, mcnt, lane, x, y, z, soft2, ax, ay, az);

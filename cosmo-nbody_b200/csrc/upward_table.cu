@@ -221,12 +221,12 @@ __global__ void __launch_bounds__(256) k_upward_table(
 // (every body and node but the root has exactly one parent), loads the
 // leaves, and then forms, round after round, every node whose two children
 // are ready; each lane owns at most two of the bucket's nodes, no lane waits
-// on another and no atomic is needed.  Every node is formed as
+// on another and no atomic is needed; the records are written afterwards,
+// consecutive nodes on consecutive lanes.  Every node is formed as
 // (left + right) of its children: the table is bit-identical to the
-// one-phase pass.  CLIMB: after every 32 buckets a warp climbs on above
-// their roots, one lane each, with the global counters (the first arrival at
-// a node stops, as in the one-phase pass); otherwise k_upward_roots does that
-// in a second launch.
+// one-phase pass.  After every 32 buckets a warp climbs on above their
+// roots, one lane each, with the global counters (the first arrival at a
+// node stops, as in the one-phase pass).
 constexpr int kUpSlots = 64;  // leaves of a bucket; its internal nodes use as many slots
 constexpr int kUpWarps = 4;
 
@@ -255,7 +255,7 @@ __device__ __forceinline__ void climb_roots(int64_t root, const int2 *__restrict
     __syncwarp();
 }
 
-template <bool QUAD, bool CLIMB>
+template <bool QUAD>
 __global__ void __launch_bounds__(kUpWarps * 32) k_upward_buckets(
     const float *__restrict__ px, const float *__restrict__ py, const float *__restrict__ pz,
     const float *__restrict__ mass, const int2 *__restrict__ children,
@@ -275,12 +275,12 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_buckets(
     if (blockIdx.x == 0 && threadIdx.x == 0 &&
         (unsigned)ws[3] != (unsigned)((uint64_t)n * (uint64_t)(n + 1) / 2))
         set_flag(status, CNB_FLAG_BAD_TOPOLOGY);
-    int64_t my_root = -1;  // CLIMB: the bucket root this lane climbs from
+    int64_t my_root = -1;  // the bucket root this lane climbs from
     const int stride = gridDim.x * kUpWarps;
     int4 bk_next = make_int4(0, 0, 0, 0);
     if (blockIdx.x * kUpWarps + w < nb) bk_next = buckets[blockIdx.x * kUpWarps + w];
     for (int g = blockIdx.x * kUpWarps + w, t = 0; g < nb; g += stride, ++t) {
-        if (CLIMB && t > 0 && (t & 31) == 0) {
+        if (t > 0 && (t & 31) == 0) {
             climb_roots<QUAD>(my_root, children, parents, counts, sums, rec, aabb, quad, n, status);
             my_root = -1;
         }
@@ -418,32 +418,9 @@ __global__ void __launch_bounds__(kUpWarps * 32) k_upward_buckets(
                              QUAD ? s_qb[w][ns] : make_float4(0.f, 0.f, 0.f, 0.f), chn[h], sums,
                              rec, aabb, quad, p == root);
         }
-        if (CLIMB && lane == (t & 31)) my_root = root;
+        if (lane == (t & 31)) my_root = root;
     }
-    if (CLIMB)
-        climb_roots<QUAD>(my_root, children, parents, counts, sums, rec, aabb, quad, n, status);
-}
-
-// Phase two: from every bucket root to the tree's root.
-template <bool QUAD>
-__global__ void __launch_bounds__(128) k_upward_roots(
-    const int2 *__restrict__ children, const int32_t *__restrict__ parents,
-    const int32_t *__restrict__ ws, int32_t *counts, float4 *sums, float4 *rec, float4 *aabb,
-    float4 *quad, int64_t n, int32_t *status) {
-    const int nb = ws[0];
-    const int4 *buckets = reinterpret_cast<const int4 *>(ws + 4);
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < nb; g += gridDim.x * blockDim.x) {
-        const int64_t root = buckets[g].z;
-        const float4 s = __ldcg(sums + root);
-        const float4 lo = __ldcg(aabb + 2 * root), hi = __ldcg(aabb + 2 * root + 1);
-        float4 qa = make_float4(0.f, 0.f, 0.f, 0.f), qb = qa;
-        if (QUAD && root >= n) {
-            qa = __ldcg(quad + 2 * root);
-            qb = __ldcg(quad + 2 * root + 1);
-        }
-        climb<QUAD>(root, s, lo, hi, qa, qb, children, parents, counts, sums, rec, aabb, quad, n,
-                    status);
-    }
+    climb_roots<QUAD>(my_root, children, parents, counts, sums, rec, aabb, quad, n, status);
 }
 
 // Reference-layout node arrays from the traversal table (octree.py:85-93
@@ -517,29 +494,17 @@ extern "C" int cnb_upward_table_quad(const float *px, const float *py, const flo
     return launch_status();
 }
 
-#ifndef CNB_UPWARD_CLIMB
-#define CNB_UPWARD_CLIMB 1
-#endif
-
 template <bool QUAD>
 static int launch_upward_buckets(const float *px, const float *py, const float *pz,
                                  const float *mass, const int2 *ch, const int32_t *parents,
                                  const int32_t *workspace, int32_t *counts, float4 *sums,
                                  float4 *rec, float4 *aabb, float4 *quad, int64_t n,
                                  int32_t *status, cudaStream_t st) {
-    constexpr bool kMode = CNB_UPWARD_CLIMB != 0;
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_upward_buckets<QUAD, kMode>,
-                                                  kUpWarps * 32, 0);
-    k_upward_buckets<QUAD, kMode><<<kSMs * (per_sm > 0 ? per_sm : 1), kUpWarps * 32, 0, st>>>(
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_upward_buckets<QUAD>, kUpWarps * 32, 0);
+    k_upward_buckets<QUAD><<<kSMs * (per_sm > 0 ? per_sm : 1), kUpWarps * 32, 0, st>>>(
         px, py, pz, mass, ch, parents, workspace, counts, sums, rec, aabb, quad, n, status);
-    CNB_TRY(launch_status());
-    if (!kMode) {
-        k_upward_roots<QUAD><<<kSMs * 4, 128, 0, st>>>(ch, parents, workspace, counts, sums, rec,
-                                                       aabb, quad, n, status);
-        CNB_TRY(launch_status());
-    }
-    return CNB_OK;
+    return launch_status();
 }
 
 extern "C" int cnb_upward_table_buckets(const float *px, const float *py, const float *pz,

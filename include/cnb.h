@@ -258,7 +258,9 @@ int cnb_build_tree_ranges(const uint64_t *codes, int32_t *children, int32_t *par
 /* Bucket table for cnb_forces_grouped (no reference counterpart): the
  * maximal subtrees holding at most max_size bodies.  workspace (device,
  * 16-byte aligned) is int32 [4 + 4N]: [0] bucket count, [1] work counter,
- * [2] deepest node stack seen by the traversal, [3] the bodies' (index + 1)
+ * [2] deepest node stack seen by the traversal (entries; for CNB_MAC_REF_X
+ * words of its stack region, one per whole-bucket entry and three per
+ * part-bucket entry, of 864), [3] the bodies' (index + 1)
  * summed over all buckets modulo 2^32 (N(N+1)/2 when the buckets tile the
  * bodies once; cnb_upward_table_buckets flags CNB_FLAG_BAD_TOPOLOGY
  * otherwise, and also when a bucket's nodes do not form a tree over its
