@@ -97,6 +97,8 @@ SIGNATURES = {
     "cnb_controller_theta": (_int, [_p, _p, _p, _i64, _p, _p, _p, _p, _int, _p]),
     "cnb_mlp_predict": (_int, [_p, _int, _p, _p, _p]),
     "cnb_mlp_grad": (_int, [_p, _p, _int, _p, _f, _p, _p, _p, _p]),
+    "cnb_mlp_grad_mma_scratch_bytes": (_i64, [_int]),
+    "cnb_mlp_grad_mma": (_int, [_p, _p, _int, _p, _f, _p, _i64, _p, _p, _p]),
     "cnb_adam_step": (_int, [_p, _p, _p, _p, _int, _f, _f, _f, _f, _int, _p]),
     "cnb_to_bf16": (_int, [_p, _p, _int, _p]),
     "cnb_colorize": (_int, [_p, _int, _int, _p, _p, _p, _p]),

@@ -58,30 +58,47 @@ class ThetaController:
     def _norm(self, X):
         return ((X - self.mean) / self.std).contiguous()
 
-    def grad(self, X, y, over_weight=4.0):
+    def _grad_fn(self, n, tensor_cores):
+        """A (X, y, g, loss, over_weight) -> None gradient call for n samples:
+        the tensor-core kernels (bfloat16 contractions, float32 accumulation)
+        or the float32 ones."""
+        if tensor_cores:
+            nbytes = int(_lib.load().cnb_mlp_grad_mma_scratch_bytes(n))
+            scratch = torch.empty((nbytes + 15) // 16, 4, dtype=torch.float32, device=self.device)
+
+            def fn(X, y, g, loss, ow):
+                _lib.call("cnb_mlp_grad_mma", X.data_ptr(), y.data_ptr(), n, self.params.data_ptr(),
+                          float(ow), scratch.data_ptr(), nbytes, g.data_ptr(), loss.data_ptr(), _st())
+        else:
+            scratch = torch.empty(4 * N_H * n + n, dtype=torch.float32, device=self.device)
+
+            def fn(X, y, g, loss, ow):
+                _lib.call("cnb_mlp_grad", X.data_ptr(), y.data_ptr(), n, self.params.data_ptr(),
+                          float(ow), scratch.data_ptr(), g.data_ptr(), loss.data_ptr(), _st())
+        return fn
+
+    def grad(self, X, y, over_weight=4.0, tensor_cores=False):
         """Loss and gradient on the GPU (libcnb kernels) for normalised features X."""
         n = X.shape[0]
-        scratch = torch.empty(4 * N_H * n + n, dtype=torch.float32, device=self.device)
         g = torch.empty(N_PARAMS, dtype=torch.float32, device=self.device)
         loss = torch.zeros(1, dtype=torch.float32, device=self.device)
-        _lib.call("cnb_mlp_grad", X.data_ptr(), y.data_ptr(), n, self.params.data_ptr(),
-                  float(over_weight), scratch.data_ptr(), g.data_ptr(), loss.data_ptr(), _st())
+        self._grad_fn(n, tensor_cores)(X, y, g, loss, over_weight)
         return loss, g
 
-    def train(self, X, y, steps=1500, lr=3e-3, over_weight=4.0, log_every=0):
-        """Full-batch Adam on (features X [n,12], labels y [n]); returns the loss curve."""
+    def train(self, X, y, steps=1500, lr=3e-3, over_weight=4.0, log_every=0, tensor_cores=True):
+        """Full-batch Adam on (features X [n,12], labels y [n]); returns the loss
+        curve.  tensor_cores: gradients from cnb_mlp_grad_mma (else cnb_mlp_grad)."""
         X = X.to(self.device, torch.float32)
         y = y.to(self.device, torch.float32).contiguous()
         self.set_normalisation(X)
         Xn = self._norm(X)
         n = Xn.shape[0]
-        scratch = torch.empty(4 * N_H * n + n, dtype=torch.float32, device=self.device)
+        grad_fn = self._grad_fn(n, tensor_cores)
         g = torch.empty(N_PARAMS, dtype=torch.float32, device=self.device)
         loss = torch.zeros(1, dtype=torch.float32, device=self.device)
         curve = []
         for it in range(steps):
-            _lib.call("cnb_mlp_grad", Xn.data_ptr(), y.data_ptr(), n, self.params.data_ptr(),
-                      float(over_weight), scratch.data_ptr(), g.data_ptr(), loss.data_ptr(), _st())
+            grad_fn(Xn, y, g, loss, over_weight)
             self.t += 1
             _lib.call("cnb_adam_step", self.params.data_ptr(), g.data_ptr(), self.m.data_ptr(),
                       self.v.data_ptr(), N_PARAMS, float(lr), 0.9, 0.999, 1e-8, self.t, _st())

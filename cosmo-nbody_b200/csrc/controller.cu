@@ -391,6 +391,301 @@ __global__ void __launch_bounds__(256) k_mlp_param_grads(
     }
 }
 
+// ---------------------------------------------------------------- training on the tensor cores
+// The same loss and gradients with the three 64-wide contractions on the
+// tensor cores (mma.sync m16n8k16, bfloat16 operands, float32 accumulation):
+// the forward second layer A2 = H1 W2^T, the backward dH1 = dA2 W2, and the
+// parameter gradients dW2 = dA2^T H1 and dW1 = dA1^T X summed over the
+// samples.  Layer 1's pre-activations, SiLU and its derivative, the loss,
+// dz, the bias sums and dw3 stay in float32.
+//
+// k_mlp_train_mma: one warp per 32 samples.  Lane s forms sample s's first
+// layer in float32 and stores H1 in bfloat16 (shared, row-major, and
+// transposed to global for the parameter GEMM); the warp runs A2 on the
+// tensor cores, finishes the forward pass and the loss on the accumulator
+// fragments, forms dA2 there, runs dH1 = dA2 W2 on the tensor cores and
+// forms dA1 (layer 1 recomputed from the staged inputs, the same fmaf
+// order as the forward pass).  dA2, dA1 and X go to global memory
+// transposed ([unit][sample], bfloat16, samples padded to a multiple of 32
+// with zero gradients).  Bias sums, dw3 and the loss are reduced in
+// registers and added once per warp.
+constexpr int kTW = 4;              // warps per block
+constexpr int kTPad = kH + 8;       // bfloat16 per row of the activation tiles
+constexpr int kTWeightBytes = (kH * kIn + 3 * kH + 4) * 4;             // w1, b1, b2, w3, b3
+constexpr int kTWarpBytes = 32 * kIn * 4 + 2 * 32 * kTPad * 2;         // inputs, H1, dA tiles
+constexpr int kTSmem = kTWeightBytes + 2 * kH * kTPad * 2 + kTW * kTWarpBytes;
+static_assert(kTWeightBytes % 16 == 0 && kTWarpBytes % 16 == 0, "16-byte aligned regions");
+
+__device__ __forceinline__ uint32_t ld_u32(const __nv_bfloat16 *p) {
+    return *reinterpret_cast<const uint32_t *>(p);
+}
+
+__global__ void __launch_bounds__(kTW * 32) k_mlp_train_mma(
+    const float *__restrict__ x, const float *__restrict__ y, int n, int n32,
+    const float *__restrict__ wg, float over_weight, __nv_bfloat16 *__restrict__ XT,
+    __nv_bfloat16 *__restrict__ H1T, __nv_bfloat16 *__restrict__ DA2T,
+    __nv_bfloat16 *__restrict__ DA1T, float *__restrict__ grad, float *__restrict__ loss) {
+    extern __shared__ __align__(16) unsigned char t_smem[];
+    float *w1 = reinterpret_cast<float *>(t_smem);
+    float *b1 = w1 + kH * kIn, *b2 = b1 + kH, *w3 = b2 + kH, *b3p = w3 + kH;
+    __nv_bfloat16 *w2 = reinterpret_cast<__nv_bfloat16 *>(t_smem + kTWeightBytes);  // [k][j]
+    __nv_bfloat16 *w2t = w2 + kH * kTPad;                                            // [j][k]
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    unsigned char *wbase = reinterpret_cast<unsigned char *>(w2t + kH * kTPad) + wib * kTWarpBytes;
+    float *sx = reinterpret_cast<float *>(wbase);                                 // [32][12]
+    __nv_bfloat16 *hid = reinterpret_cast<__nv_bfloat16 *>(wbase + 32 * kIn * 4);  // [32][kTPad]
+    __nv_bfloat16 *dbuf = hid + 32 * kTPad;                                       // [32][kTPad]
+    for (int i = threadIdx.x; i < kH * kIn; i += blockDim.x) w1[i] = wg[kOffW1 + i];
+    for (int i = threadIdx.x; i < kH; i += blockDim.x) {
+        b1[i] = wg[kOffB1 + i];
+        b2[i] = wg[kOffB2 + i];
+        w3[i] = wg[kOffW3 + i];
+    }
+    if (threadIdx.x == 0) b3p[0] = wg[kOffB3];
+    for (int i = threadIdx.x; i < kH * kH; i += blockDim.x) {
+        const int k = i / kH, j = i % kH;
+        const __nv_bfloat16 v = __float2bfloat16_rn(wg[kOffW2 + i]);
+        w2[k * kTPad + j] = v;
+        w2t[j * kTPad + k] = v;
+    }
+    __syncthreads();
+    const float b3 = b3p[0];
+    float acc_b1[16], acc_b2[16], acc_w3[16];  // column nt * 8 + tig * 2 + e at index 2 nt + e
+#pragma unroll
+    for (int c = 0; c < 16; ++c) acc_b1[c] = acc_b2[c] = acc_w3[c] = 0.f;
+    float acc_b3 = 0.f, lsum = 0.f;
+    for (int base = (blockIdx.x * kTW + wib) * 32; base < n32; base += gridDim.x * kTW * 32) {
+        const int s = base + lane;
+        // layer 1, one sample per lane, float32
+        float xv[kIn];
+#pragma unroll
+        for (int i = 0; i < kIn; ++i) {
+            xv[i] = s < n ? x[(int64_t)s * kIn + i] : 0.f;
+            sx[lane * kIn + i] = xv[i];
+        }
+#pragma unroll
+        for (int i = 0; i < 16; ++i) XT[(int64_t)i * n32 + s] = __float2bfloat16_rn(i < kIn ? xv[i] : 0.f);
+#pragma unroll 4
+        for (int j = 0; j < kH; j += 2) {
+            float a0 = b1[j], a1 = b1[j + 1];
+#pragma unroll
+            for (int i = 0; i < kIn; ++i) {
+                a0 = fmaf(w1[j * kIn + i], xv[i], a0);
+                a1 = fmaf(w1[(j + 1) * kIn + i], xv[i], a1);
+            }
+            const __nv_bfloat162 hb = __floats2bfloat162_rn(siluf_(a0), siluf_(a1));
+            *reinterpret_cast<__nv_bfloat162 *>(hid + lane * kTPad + j) = hb;
+            H1T[(int64_t)j * n32 + s] = hb.x;
+            H1T[(int64_t)(j + 1) * n32 + s] = hb.y;
+        }
+        __syncwarp();
+        // per 16-sample row tile: A2 = H1 W2^T on the tensor cores (rows =
+        // samples, columns = units), z, the loss, dz and dA2 on the fragments
+#pragma unroll 1
+        for (int mt = 0; mt < 2; ++mt) {
+            float d[8][4];
+            {
+                uint32_t a[4][4];
+                const __nv_bfloat16 *r0 = hid + (mt * 16 + gid) * kTPad, *r1 = r0 + 8 * kTPad;
+#pragma unroll
+                for (int kt = 0; kt < 4; ++kt) {
+                    const int c = kt * 16 + tig * 2;
+                    a[kt][0] = ld_u32(r0 + c);
+                    a[kt][1] = ld_u32(r1 + c);
+                    a[kt][2] = ld_u32(r0 + c + 8);
+                    a[kt][3] = ld_u32(r1 + c + 8);
+                }
+#pragma unroll
+                for (int nt = 0; nt < 8; ++nt) {
+                    d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
+                    const __nv_bfloat16 *wr = w2 + (nt * 8 + gid) * kTPad;
+#pragma unroll
+                    for (int kt = 0; kt < 4; ++kt) {
+                        const int c = kt * 16 + tig * 2;
+                        const uint32_t b[2] = {ld_u32(wr + c), ld_u32(wr + c + 8)};
+                        mma_bf16_16816(d[nt], a[kt], b);
+                    }
+                }
+            }
+            // z per sample: the four lanes of a row group hold its partial sums
+            float zp[2] = {0.f, 0.f};
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int col = nt * 8 + tig * 2 + (e & 1);
+                    d[nt][e] += b2[col];
+                    zp[e >> 1] = fmaf(w3[col], siluf_(d[nt][e]), zp[e >> 1]);
+                }
+            float dzr[2];
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                float z = zp[q];
+                z += __shfl_xor_sync(0xffffffffu, z, 1);
+                z += __shfl_xor_sync(0xffffffffu, z, 2);
+                z += b3;
+                const int sr = base + mt * 16 + gid + 8 * q;
+                float dz = 0.f;
+                if (sr < n) {
+                    const float sg = sigmoidf_(z);
+                    const float diff = kThetaLo + (kThetaHi - kThetaLo) * sg - y[sr];
+                    const float c = diff > 0.f ? over_weight : 1.f;
+                    if (tig == 0) lsum += c * diff * diff;
+                    dz = (2.f * c * diff / (float)n) * (kThetaHi - kThetaLo) * sg * (1.f - sg);
+                }
+                dzr[q] = dz;
+                if (tig == 0) acc_b3 += dz;
+            }
+            // dA2 on the fragments; dw3 and db2 sums
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int col = nt * 8 + tig * 2 + (e & 1);
+                    const float a2 = d[nt][e], dz = dzr[e >> 1];
+                    const float sa = sigmoidf_(a2);
+                    acc_w3[2 * nt + (e & 1)] = fmaf(dz, a2 * sa, acc_w3[2 * nt + (e & 1)]);
+                    d[nt][e] = dz * w3[col] * sa * (1.f + a2 * (1.f - sa));
+                    acc_b2[2 * nt + (e & 1)] += d[nt][e];
+                }
+                const int r = mt * 16 + gid, c = nt * 8 + tig * 2;
+                *reinterpret_cast<__nv_bfloat162 *>(dbuf + r * kTPad + c) =
+                    __floats2bfloat162_rn(d[nt][0], d[nt][1]);
+                *reinterpret_cast<__nv_bfloat162 *>(dbuf + (r + 8) * kTPad + c) =
+                    __floats2bfloat162_rn(d[nt][2], d[nt][3]);
+            }
+        }
+        __syncwarp();
+        for (int k = 0; k < kH; ++k) DA2T[(int64_t)k * n32 + s] = dbuf[lane * kTPad + k];
+        // per row tile: dH1 = dA2 W2 on the tensor cores, then dA1 = dH1 * SiLU'(A1)
+        // with A1 recomputed from the staged inputs (the forward pass's fmaf order)
+#pragma unroll 1
+        for (int mt = 0; mt < 2; ++mt) {
+            float d[8][4];
+            {
+                uint32_t a[4][4];
+                const __nv_bfloat16 *r0 = dbuf + (mt * 16 + gid) * kTPad, *r1 = r0 + 8 * kTPad;
+#pragma unroll
+                for (int kt = 0; kt < 4; ++kt) {
+                    const int c = kt * 16 + tig * 2;
+                    a[kt][0] = ld_u32(r0 + c);
+                    a[kt][1] = ld_u32(r1 + c);
+                    a[kt][2] = ld_u32(r0 + c + 8);
+                    a[kt][3] = ld_u32(r1 + c + 8);
+                }
+                __syncwarp();  // this tile's dA2 is read by every lane before dA1 overwrites it
+#pragma unroll
+                for (int nt = 0; nt < 8; ++nt) {
+                    d[nt][0] = d[nt][1] = d[nt][2] = d[nt][3] = 0.f;
+                    const __nv_bfloat16 *wr = w2t + (nt * 8 + gid) * kTPad;
+#pragma unroll
+                    for (int kt = 0; kt < 4; ++kt) {
+                        const int c = kt * 16 + tig * 2;
+                        const uint32_t b[2] = {ld_u32(wr + c), ld_u32(wr + c + 8)};
+                        mma_bf16_16816(d[nt], a[kt], b);
+                    }
+                }
+            }
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int r = mt * 16 + gid + 8 * (e >> 1), j = nt * 8 + tig * 2 + (e & 1);
+                    float a1 = b1[j];
+#pragma unroll
+                    for (int i = 0; i < kIn; ++i) a1 = fmaf(w1[j * kIn + i], sx[r * kIn + i], a1);
+                    const float sa = sigmoidf_(a1);
+                    d[nt][e] *= sa * (1.f + a1 * (1.f - sa));
+                    acc_b1[2 * nt + (e & 1)] += d[nt][e];
+                }
+                const int r = mt * 16 + gid, c = nt * 8 + tig * 2;
+                *reinterpret_cast<__nv_bfloat162 *>(dbuf + r * kTPad + c) =
+                    __floats2bfloat162_rn(d[nt][0], d[nt][1]);
+                *reinterpret_cast<__nv_bfloat162 *>(dbuf + (r + 8) * kTPad + c) =
+                    __floats2bfloat162_rn(d[nt][2], d[nt][3]);
+            }
+        }
+        __syncwarp();
+        for (int j = 0; j < kH; ++j) DA1T[(int64_t)j * n32 + s] = dbuf[lane * kTPad + j];
+        __syncwarp();
+    }
+    // column sums over the eight row groups of the warp, one atomic per column
+#pragma unroll
+    for (int c = 0; c < 16; ++c) {
+        float v1 = acc_b1[c], v2 = acc_b2[c], v3 = acc_w3[c];
+#pragma unroll
+        for (int o = 4; o < 32; o <<= 1) {
+            v1 += __shfl_xor_sync(0xffffffffu, v1, o);
+            v2 += __shfl_xor_sync(0xffffffffu, v2, o);
+            v3 += __shfl_xor_sync(0xffffffffu, v3, o);
+        }
+        if (gid == 0) {
+            const int col = (c >> 1) * 8 + tig * 2 + (c & 1);
+            atomicAdd(grad + kOffB1 + col, v1);
+            atomicAdd(grad + kOffB2 + col, v2);
+            atomicAdd(grad + kOffW3 + col, v3);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        acc_b3 += __shfl_xor_sync(0xffffffffu, acc_b3, o);
+        lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
+    }
+    if (lane == 0) {
+        atomicAdd(grad + kOffB3, acc_b3);
+        atomicAdd(loss, lsum / (float)n);
+    }
+}
+
+// dW2 = dA2^T H1 (64 x 64) and dW1 = dA1^T X (64 x 12, X padded to 16) over
+// the samples of one chunk per block, on the tensor cores.  Warp w takes
+// row tile w & 3 of both outputs, column tiles 4 (w >> 2) .. + 3 of dW2 and
+// column tile w >> 2 of dW1; both operands are read from the transposed
+// [unit][sample] arrays, so every fragment register is two consecutive
+// samples.  Partial sums are added into grad.
+constexpr int kPW = 8;
+__global__ void __launch_bounds__(kPW * 32) k_mlp_param_mma(
+    const __nv_bfloat16 *__restrict__ XT, const __nv_bfloat16 *__restrict__ H1T,
+    const __nv_bfloat16 *__restrict__ DA2T, const __nv_bfloat16 *__restrict__ DA1T, int n32,
+    int chunk, float *__restrict__ grad) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int gid = lane >> 2, tig = lane & 3;
+    const int mt = w & 3, nq = w >> 2;
+    const int k_begin = blockIdx.x * chunk, k_end = min(n32, k_begin + chunk);
+    float c2[4][4], c1[4] = {0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) c2[q][0] = c2[q][1] = c2[q][2] = c2[q][3] = 0.f;
+    const __nv_bfloat16 *a2r0 = DA2T + (int64_t)(mt * 16 + gid) * n32, *a2r1 = a2r0 + 8LL * n32;
+    const __nv_bfloat16 *a1r0 = DA1T + (int64_t)(mt * 16 + gid) * n32, *a1r1 = a1r0 + 8LL * n32;
+    const __nv_bfloat16 *xr = XT + (int64_t)(nq * 8 + gid) * n32;
+    for (int k0 = k_begin; k0 < k_end; k0 += 16) {
+        const int c = k0 + tig * 2;
+        const uint32_t a[4] = {ld_u32(a2r0 + c), ld_u32(a2r1 + c), ld_u32(a2r0 + c + 8),
+                               ld_u32(a2r1 + c + 8)};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const __nv_bfloat16 *hr = H1T + (int64_t)((nq * 4 + q) * 8 + gid) * n32;
+            const uint32_t b[2] = {ld_u32(hr + c), ld_u32(hr + c + 8)};
+            mma_bf16_16816(c2[q], a, b);
+        }
+        const uint32_t a1[4] = {ld_u32(a1r0 + c), ld_u32(a1r1 + c), ld_u32(a1r0 + c + 8),
+                                ld_u32(a1r1 + c + 8)};
+        const uint32_t b1[2] = {ld_u32(xr + c), ld_u32(xr + c + 8)};
+        mma_bf16_16816(c1, a1, b1);
+    }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int row = mt * 16 + gid + 8 * (e >> 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int col = (nq * 4 + q) * 8 + tig * 2 + (e & 1);
+            atomicAdd(grad + kOffW2 + row * kH + col, c2[q][e]);
+        }
+        const int col1 = nq * 8 + tig * 2 + (e & 1);
+        if (col1 < kIn) atomicAdd(grad + kOffW1 + row * kIn + col1, c1[e]);
+    }
+}
+
 __global__ void k_adam(float *__restrict__ p, const float *__restrict__ g, float *__restrict__ m,
                        float *__restrict__ v, int n, float lr, float b1, float b2, float eps,
                        float c1, float c2) {
@@ -464,6 +759,42 @@ extern "C" int cnb_mlp_grad(const float *features, const float *labels, int n,
         features, labels, n, weights, over_weight, H1, DA1, H2, DA2, DZ, loss);
     CNB_TRY(launch_status());
     k_mlp_param_grads<<<2 * kH + 1, 256, 0, st>>>(features, n, H1, DA1, H2, DA2, DZ, grad);
+    return launch_status();
+}
+
+extern "C" int64_t cnb_mlp_grad_mma_scratch_bytes(int n) {
+    if (n < 1) return -1;
+    const int64_t n32 = ((int64_t)n + 31) / 32 * 32;
+    return (16 + 3 * kH) * n32 * (int64_t)sizeof(__nv_bfloat16);
+}
+
+extern "C" int cnb_mlp_grad_mma(const float *features, const float *labels, int n,
+                                const float *weights, float over_weight, void *scratch,
+                                int64_t scratch_bytes, float *grad, float *loss, void *stream) {
+    if (n < 1 || !features || !labels || !weights || !scratch || !grad || !loss)
+        return CNB_E_INVALID_ARG;
+    if ((reinterpret_cast<uintptr_t>(scratch) & 15) != 0 ||
+        scratch_bytes < cnb_mlp_grad_mma_scratch_bytes(n))
+        return CNB_E_INVALID_ARG;
+    if (n > (1 << 28)) return CNB_E_TOO_LARGE;
+    cudaStream_t st = as_stream(stream);
+    const int n32 = (n + 31) / 32 * 32;
+    __nv_bfloat16 *XT = static_cast<__nv_bfloat16 *>(scratch);
+    __nv_bfloat16 *H1T = XT + 16LL * n32, *DA2T = H1T + (int64_t)kH * n32,
+                  *DA1T = DA2T + (int64_t)kH * n32;
+    CNB_CUDA(cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st));
+    CNB_CUDA(cudaMemsetAsync(loss, 0, sizeof(float), st));
+    CNB_CUDA(cudaFuncSetAttribute(k_mlp_train_mma, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  kTSmem));
+    const int tiles = n32 / 32;
+    const int blocks = (tiles + kTW - 1) / kTW < 148 * 2 ? (tiles + kTW - 1) / kTW : 148 * 2;
+    k_mlp_train_mma<<<blocks, kTW * 32, kTSmem, st>>>(features, labels, n, n32, weights,
+                                                       over_weight, XT, H1T, DA2T, DA1T, grad,
+                                                       loss);
+    CNB_TRY(launch_status());
+    constexpr int kChunk = 1024;
+    k_mlp_param_mma<<<(n32 + kChunk - 1) / kChunk, kPW * 32, 0, st>>>(XT, H1T, DA2T, DA1T, n32,
+                                                                      kChunk, grad);
     return launch_status();
 }
 

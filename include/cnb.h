@@ -502,6 +502,18 @@ int cnb_mlp_predict(const float *features, int n, const float *weights, float *t
 int cnb_mlp_grad(const float *features, const float *labels, int n, const float *weights,
                  float over_weight, float *scratch, float *grad, float *loss, void *stream);
 
+/* cnb_mlp_grad with the three 64-wide contractions on the tensor cores
+ * (mma.sync m16n8k16, bfloat16 operands, float32 accumulation): the forward
+ * second layer, the backward dH1 = dA2 W2 and the parameter gradients dW2 =
+ * dA2^T H1 and dW1 = dA1^T X over the samples; layer 1, the activations'
+ * derivatives, the loss, the bias sums and dw3 stay in float32.  scratch:
+ * device, 16-byte aligned, at least cnb_mlp_grad_mma_scratch_bytes(n)
+ * bytes (bfloat16 activations, transposed). */
+int64_t cnb_mlp_grad_mma_scratch_bytes(int n);
+int cnb_mlp_grad_mma(const float *features, const float *labels, int n, const float *weights,
+                     float over_weight, void *scratch, int64_t scratch_bytes, float *grad,
+                     float *loss, void *stream);
+
 /* One Adam update of n parameters (step t >= 1). */
 int cnb_adam_step(float *params, const float *grad, float *m, float *v, int n, float lr,
                   float beta1, float beta2, float eps, int t, void *stream);

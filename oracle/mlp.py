@@ -82,6 +82,40 @@ def loss_and_grad(p, X, y, over_weight=1.0):
     return loss, g
 
 
+def loss_and_grad_tc(p, X, y, over_weight=1.0):
+    """Loss and gradient of the tensor-core training path: the operands of
+    the four 64-wide contractions rounded to bfloat16 (H1 and W2 in the
+    forward second layer, dA2 and W2 in dH1 = dA2 W2, dA2 and H1 in dW2, dA1
+    and X in dW1), everything else in float64."""
+    W1, b1, W2, b2, w3, b3 = unpack(p)
+    X = np.asarray(X, np.float64)
+
+    def bf(a):
+        return bf16_round(np.asarray(a, np.float32)).astype(np.float64)
+    a1 = X @ W1.T + b1
+    h1b, W2b = bf(silu(a1)), bf(W2)
+    a2 = h1b @ W2b.T + b2
+    h2 = silu(a2)
+    z = h2 @ w3 + b3
+    theta = THETA_LO + (THETA_HI - THETA_LO) * sigmoid(z)
+    n = X.shape[0]
+    diff = theta - np.asarray(y, np.float64)
+    c = np.where(diff > 0, over_weight, 1.0)
+    loss = float(np.mean(c * diff * diff))
+    sg = sigmoid(z)
+    dz = 2.0 * c * diff / n * (THETA_HI - THETA_LO) * sg * (1.0 - sg)
+    g = np.zeros(N_PARAMS)
+    g[OFF_W3:OFF_B3] = dz @ h2
+    g[OFF_B3] = dz.sum()
+    da2 = np.outer(dz, w3) * dsilu(a2)
+    g[OFF_W2:OFF_B2] = (bf(da2).T @ h1b).ravel()
+    g[OFF_B2:OFF_W3] = da2.sum(axis=0)
+    da1 = (bf(da2) @ W2b) * dsilu(a1)
+    g[OFF_W1:OFF_B1] = (bf(da1).T @ bf(X)).ravel()
+    g[OFF_B1:OFF_W2] = da1.sum(axis=0)
+    return loss, g
+
+
 def bf16_round(a):
     """float32 -> bfloat16 -> float32, round to nearest even."""
     a = np.ascontiguousarray(a, np.float32)

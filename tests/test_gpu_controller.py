@@ -43,6 +43,40 @@ def test_gpu_gradient_matches_oracle():
         assert rel < 1e-4, (lo, rel)
 
 
+@pytest.mark.parametrize("n", [1000, 1003, 70000])
+def test_tensor_core_gradient_matches_oracle(n):
+    """cnb_mlp_grad_mma (bf16 tensor-core contractions, float32 accumulation)
+    against the float64 oracle with the same operands rounded to bf16, and
+    against the exact float64 gradient; n not a multiple of 32 pads with
+    samples of zero gradient."""
+    from cnb import _lib
+    rng = np.random.default_rng(7)
+    p = (rng.standard_normal(mlp.N_PARAMS) * 0.3).astype(np.float32)
+    X = rng.standard_normal((n, mlp.N_IN)).astype(np.float32)
+    y = rng.uniform(0.2, 1.0, n).astype(np.float32)
+    P, Xd, yd = (torch.from_numpy(a).cuda() for a in (p, X, y))
+    nbytes = int(_lib.load().cnb_mlp_grad_mma_scratch_bytes(n))
+    assert nbytes >= 208 * 2 * n
+    scratch = torch.empty(nbytes // 4 + 4, device="cuda")
+    g = torch.full((mlp.N_PARAMS,), 7.0, device="cuda")   # overwritten, not accumulated into
+    loss = torch.full((1,), 7.0, device="cuda")
+    _lib.call("cnb_mlp_grad_mma", Xd.data_ptr(), yd.data_ptr(), n, P.data_ptr(), 3.0,
+              scratch.data_ptr(), nbytes, g.data_ptr(), loss.data_ptr(), st())
+    gg = g.cpu().numpy().astype(np.float64)
+    tl, tg = mlp.loss_and_grad_tc(p.astype(np.float64), X, y, over_weight=3.0)
+    el, eg = mlp.loss_and_grad(p.astype(np.float64), X, y, over_weight=3.0)
+    assert abs(loss.item() - tl) <= 1e-5 * max(1.0, tl)
+    for lo, hi in ((mlp.OFF_W1, mlp.OFF_B1), (mlp.OFF_B1, mlp.OFF_W2), (mlp.OFF_W2, mlp.OFF_B2),
+                   (mlp.OFF_B2, mlp.OFF_W3), (mlp.OFF_W3, mlp.OFF_B3), (mlp.OFF_B3, mlp.N_PARAMS)):
+        rel_tc = np.linalg.norm(gg[lo:hi] - tg[lo:hi]) / np.linalg.norm(tg[lo:hi])
+        rel_ex = np.linalg.norm(gg[lo:hi] - eg[lo:hi]) / np.linalg.norm(eg[lo:hi])
+        assert rel_tc < 2e-3, (lo, rel_tc)      # the same bf16 operands: float32 sums only
+        assert rel_ex < 3e-2, (lo, rel_ex)      # bf16 operands against exact float64
+    with pytest.raises(_lib.CnbError):
+        _lib.call("cnb_mlp_grad_mma", Xd.data_ptr(), yd.data_ptr(), n, P.data_ptr(), 3.0,
+                  scratch.data_ptr(), nbytes - 16, g.data_ptr(), loss.data_ptr(), st())
+
+
 def test_predict_matches_oracle_forward():
     from cnb import _lib
     rng = np.random.default_rng(1)
