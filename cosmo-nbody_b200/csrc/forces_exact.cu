@@ -564,7 +564,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             // keeps item j's mask of opening bodies, and the children of every
             // item that some body opened are pushed together afterwards
             uint2 my_om = make_uint2(0u, 0u);
-#pragma unroll 2
+#pragma unroll 1
             for (int j = 0; j < pcnt; ++j) {
                 const float4 I = plist[3 * j], J = plist[3 * j + 1], K = plist[3 * j + 2];
                 bool opn[BPL];
