@@ -224,26 +224,33 @@ def measured_peaks():
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 
-def fma_peak_tflops():
-    """Measured FP32 FMA throughput (libcnb probe), TFLOP/s."""
+def fma_peak_tflops(detail=None):
+    """Measured FP32 FMA throughput (libcnb probes), TFLOP/s: the higher of
+    scalar FFMA chains and packed FFMA2 chains (the force loops issue FFMA2).
+    detail (dict, optional) receives both figures."""
     import torch
     from cnb import _lib
     blocks = 148 * 16
     out = torch.empty(blocks * 256, dtype=torch.float32, device="cuda")
     iters = 20000
     st = int(torch.cuda.current_stream().cuda_stream)
-    for _ in range(2):
-        _lib.call("cnb_fma_probe", out.data_ptr(), iters, blocks, st)
-    best = 0.0
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        _lib.call("cnb_fma_probe", out.data_ptr(), iters, blocks, st)
-        e1.record()
-        e1.synchronize()
-        ms = e0.elapsed_time(e1)
-        best = max(best, 16.0 * iters * blocks * 256 / (ms * 1e-3) / 1e12)
-    return best
+    res = {}
+    for name, flops_per_iter in (("cnb_fma_probe", 16.0), ("cnb_fma2_probe", 32.0)):
+        for _ in range(2):
+            _lib.call(name, out.data_ptr(), iters, blocks, st)
+        best = 0.0
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            _lib.call(name, out.data_ptr(), iters, blocks, st)
+            e1.record()
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            best = max(best, flops_per_iter * iters * blocks * 256 / (ms * 1e-3) / 1e12)
+        res["ffma" if name == "cnb_fma_probe" else "ffma2"] = best
+    if detail is not None:
+        detail.update(res)
+    return max(res.values())
 
 
 # ---------------------------------------------------------------- CPU (reference algorithm)
@@ -600,7 +607,8 @@ def run_ours(args):
         line["interactions_per_body"] = interactions_per_step / n
 
     if not args.profile:
-        peak = fma_peak_tflops()
+        probes = {}
+        peak = fma_peak_tflops(probes)
         achieved = interactions_per_step * FLOPS_PER_INTERACTION / (forces_ms * 1e-3) / 1e12
         traffic = FORCES_TRAFFIC_BYTES_128.get(args.mac) if (
             args.n_grid == 128 and abs(args.theta - 0.5) < 1e-9 and args.force_mode == "grouped") else None
@@ -613,7 +621,9 @@ def run_ours(args):
                             "traffic_source": "ncu capture of this kernel on this workload (one launch, "
                                               "64-body buckets, 512-body super-buckets), not this run"
                                               if traffic else None,
-                            "note": "peak = measured FP32 FMA throughput (cnb_fma_probe); "
+                            "peak_probes_tflops": probes,
+                            "note": "peak = measured FP32 FMA throughput, the higher of scalar FFMA "
+                                    "(cnb_fma_probe) and packed FFMA2 (cnb_fma2_probe) chains; "
                                     f"{FLOPS_PER_INTERACTION} flops per body-node interaction; "
                                     "interactions = the accepted (body, node) pairs counted on the device"}
         line["clocks"] = sampler.summary()

@@ -533,6 +533,8 @@ int cnb_direct_sum_f64(const float *px, const float *py, const float *pz, const 
 /* FP32 FMA throughput probe (no reference counterpart): `blocks` x 256
  * threads, 16 * iters flops per thread; out holds blocks*256 floats. */
 int cnb_fma_probe(float *out, int64_t iters, int blocks, void *stream);
+/* The same with packed float2 FMAs (FFMA2): 32 flops per thread per iteration. */
+int cnb_fma2_probe(float *out, int64_t iters, int blocks, void *stream);
 
 #ifdef __cplusplus
 }
