@@ -1,5 +1,5 @@
 """The CPU oracle of the controller network: its analytic gradient against
-central finite differences (float64), so it can judge the GPU kernels."""
+central finite differences (float64), so it can check the GPU kernels."""
 import numpy as np
 
 from oracle import mlp
