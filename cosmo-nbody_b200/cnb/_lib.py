@@ -114,6 +114,7 @@ SIGNATURES = {
     "cnb_direct_sum_f64": (_int, [_p, _p, _p, _p, _i64, _p, _i64, _d, _d, _p, _p]),
     "cnb_fma_probe": (_int, [_p, _i64, _int, _p]),
     "cnb_fma2_probe": (_int, [_p, _i64, _int, _p]),
+    "cnb_exact_test_spill": (_int, [_int]),
 }
 
 _lib = None

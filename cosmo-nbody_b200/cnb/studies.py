@@ -111,7 +111,7 @@ def precision(args):
                 if upward == "compensated":
                     r = eng.tree_manager.root_f64.cpu().numpy()
                     out["root_mass_f64"] = float(r[0])
-                out["root_mass_f32"] = float(eng.tree_manager.mass[n].item())
+                out["root_mass_f32"] = float(eng.tree_manager.get_buffers()["mass"][n].item())
                 print(json.dumps(out), flush=True)
     # upward-pass error against float64 sums on a sample of internal nodes
     st = SimulationState(n, pos, vel)
@@ -131,8 +131,9 @@ def precision(args):
             return c[hi] - torch.where(lo > 0, c[(lo - 1).clamp_min(0)], torch.zeros_like(c[hi]))
         mref = seg(cm)
         cref = torch.stack([seg(c) / mref for c in cs], 1)
-        merr = ((tm.mass[nodes].double() - mref).abs() / mref).max().item()
-        cerr = (tm.get_buffers()["com"][nodes].double() - cref).abs().max().item()
+        buf = tm.get_buffers()  # the reference-layout arrays (filled from the node table)
+        merr = ((buf["mass"][nodes].double() - mref).abs() / mref).max().item()
+        cerr = (buf["com"][nodes].double() - cref).abs().max().item()
         print(json.dumps(dict(study="upward", n_grid=args.n_grid, upward=upward,
                               max_rel_mass_err=merr, max_abs_com_err=cerr,
                               nodes_checked=int(nodes.numel()))), flush=True)

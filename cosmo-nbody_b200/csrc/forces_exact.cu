@@ -50,15 +50,21 @@ namespace cnb {
 
 constexpr float kCutLo = 0.99999e-7f, kCutHi = 1.00001e-7f;  // float64 band around the cut
 
-// The two node stacks of a warp share one region of kXWords words: entries
+// The two node stacks of a warp share one region of XW words: entries
 // reached by the whole bucket (one word, the node) grow up from word 0,
 // entries reached by part of it (three words: node, mask low, mask high)
-// grow down from the end; a push that would make them meet drops the
-// children and flags CNB_FLAG_LIST_OVERFLOW.  The deepest use measured on
-// 128^3 and 256^3 Zel'dovich and evolved states (two-level walk included) is
-// 568 words; 864 is the most that keeps ten 2-warp blocks (20 warps) per SM.
-constexpr int kXWords = 864;
-__device__ __forceinline__ int part_word(int k) { return kXWords - 3 * (k + 1); }
+// grow down from the end.  The main pass gives up on a bucket whose stacks
+// would meet (it marks the bucket's record and writes no force for it); a
+// second pass walks only those buckets again with a region of
+// kXWordsRedo words, and a push that would overflow that one drops the
+// children and flags CNB_FLAG_LIST_OVERFLOW.  The deepest use measured at
+// theta = 0.5 on 128^3 and 256^3 Zel'dovich and evolved states (two-level
+// walk included) is 568 words; 864 is the most that keeps ten 2-warp
+// blocks (20 warps) per SM; smaller angles walk deeper and start wider.
+constexpr int kXWords = 864;       // main pass, theta >= 0.4
+constexpr int kXWordsWide = 2048;  // main pass, theta < 0.4
+constexpr int kXWordsRedo = 4096;  // the buckets a main pass gave up on
+template <int XW> __device__ __forceinline__ int part_word(int k) { return XW - 3 * (k + 1); }
 
 // per-warp shared memory: the whole-bucket and masked lists (packed for two
 // bodies per lane), the per-pair list (one float4 per entry), the per-body
@@ -69,9 +75,9 @@ template <int BPL> __host__ __device__ constexpr int exact_f4_per_warp() {
 constexpr int kExactMasksPerWarp = 2 * kGList;  // uint2
 
 template <int BPL>
-constexpr size_t exact_smem(int warps) {
+constexpr size_t exact_smem(int warps, int xw) {
     return (size_t)warps * (exact_f4_per_warp<BPL>() * sizeof(float4) +
-                            kExactMasksPerWarp * sizeof(uint2) + kXWords * sizeof(int32_t));
+                            kExactMasksPerWarp * sizeof(uint2) + xw * sizeof(int32_t));
 }
 
 // per-body item flags
@@ -307,8 +313,13 @@ __device__ __forceinline__ void flush32(float4 *lst, uint2 *msk, int &cnt, int l
     __syncwarp();
 }
 
-template <int BPL, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
+// REDO false: the main pass over every bucket (work counter); true: the
+// buckets a main pass gave up on (bucket record's fourth word = 1), found by
+// a strided scan of the table and cleared when done.
+// Twenty warps per SM: ten 2-warp blocks fit the shared memory of the main
+// pass; the register bound (at most 102 for 2 or 4 warps per block) keeps them.
+template <int BPL, int WARPS, int XW, bool REDO, bool TEST = false>
+__global__ void __launch_bounds__(WARPS * 32, 20 / WARPS) k_forces_exact(GroupedParams P) {
     static_assert(BPL == 1 || BPL == 2, "one or two bodies per lane");
     extern __shared__ __align__(16) unsigned char x_smem[];
     constexpr int EW = entry_width<BPL>();
@@ -324,7 +335,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
     uint2 *xmask = mmask + kGList;
     // the stack region: whole-bucket entries from word 0 up, (node, mask) entries from the end down
     int32_t *stack = reinterpret_cast<int32_t *>(mbase + WARPS * kExactMasksPerWarp) +
-                     wib * kXWords;
+                     wib * XW;
 
     unsigned long long n_tests = 0, n_inter = 0, n_wrap = 0;
     int max_top = 0;
@@ -332,13 +343,32 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
     const int n_buckets = P.ws[0];
     const float half_box = 0.5f * P.box;
 
+    int4 *table = reinterpret_cast<int4 *>(P.ws + 4);  // the bucket records (P.buckets)
+    // redo: this warp's share of the table, 32 records at a time (lane l reads record
+    // chunk + l); marked holds the records of the chunk still to walk
+    int chunk = (blockIdx.x * WARPS + wib) * 32;
+    uint32_t marked = 0u;
     for (;;) {
         int g = 0;
-        if (lane == 0) g = atomicAdd(P.ws + 1, 1);
-        g = __shfl_sync(0xffffffffu, g, 0);
-        if (g >= n_buckets) break;
-        if (P.bucket_order) g = P.bucket_order[g];
+        if (REDO) {
+            while (marked == 0u && chunk < n_buckets) {
+                const int r = chunk + lane;
+                marked = __ballot_sync(0xffffffffu, r < n_buckets && table[r].w == 1);
+                if (marked == 0u) chunk += gridDim.x * WARPS * 32;
+            }
+            if (marked == 0u) break;
+            g = chunk + __ffs(marked) - 1;
+            marked &= marked - 1u;
+            if (marked == 0u) chunk += gridDim.x * WARPS * 32;
+        } else {
+            if (lane == 0) g = atomicAdd(P.ws + 1, 1);
+            g = __shfl_sync(0xffffffffu, g, 0);
+            if (g >= n_buckets) break;
+            if (P.bucket_order) g = P.bucket_order[g];
+        }
         const int4 bk = P.buckets[g];
+        bool spill = false;  // main pass: this bucket is left to the redo pass
+        uint32_t b_tests = 0, b_inter = 0, b_wrap = 0;  // this bucket's counts (lane's share)
         const int count = bk.y;
         float x[BPL], y[BPL], z[BPL];
         bool valid[BPL];
@@ -404,7 +434,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
         if (P.super_of_body) {
             const int sup = P.super_of_body[bk.x];
             const int4 h = sup >= 0 ? P.super_hdr[sup] : make_int4(0, 0, 0, 0);
-            if (h.w && h.z <= kXWords) {
+            if (h.w && h.z <= XW) {
                 // the nodes every body of the super-bucket accepts (k_super_lists)
                 const float4 *far = P.far_lists + (int64_t)sup * P.far_cap;
                 for (int j0 = 0; j0 < h.x; j0 += 32) {
@@ -422,8 +452,8 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                     __syncwarp();
                 }
                 if (lane == 0) {
-                    n_inter += (unsigned long long)(h.x + h.y) * count;
-                    n_wrap += (unsigned long long)h.y * count;
+                    b_inter += (uint32_t)((h.x + h.y) * count);
+                    b_wrap += (uint32_t)(h.y * count);
                 }
                 const int32_t *near = P.near_lists + (int64_t)sup * P.near_cap;
                 for (int j = lane; j < h.z; j += 32) stack[j] = near[j];
@@ -434,7 +464,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
         if (!seeded && lane == 0) stack[0] = root;
         __syncwarp();
         int64_t rounds = 0;
-        while (top > 0 || ptop > 0) {
+        while ((top > 0 || ptop > 0) && !spill) {
             // a valid tree pushes every node at most once per bucket
             if (++rounds > P.m_nodes) {
                 if (lane == 0) set_flag(P.status, CNB_FLAG_BAD_TOPOLOGY);
@@ -448,7 +478,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             int32_t node = -1;
             uint2 mk = fm;
             if (lane < k1) {
-                const int pw = part_word(ptop + lane);
+                const int pw = part_word<XW>(ptop + lane);
                 node = stack[pw];
                 mk = make_uint2((uint32_t)stack[pw + 1], (uint32_t)stack[pw + 2]);
             } else if (lane < k1 + k2) {
@@ -496,7 +526,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                     E = make_float4(A.x - sx_, A.y - sy_, A.z - sz_, A.w);
                 }
             }
-            n_tests += (node >= 0);
+            b_tests += (node >= 0);
             const bool to_list = cls == 1 && whole && one_image && !near_box;
             const bool to_m = cls == 1 && !whole && one_image && !near_box;
             const bool to_x = cls == 1 && !(one_image && !near_box);
@@ -508,7 +538,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             const uint32_t m_pb = __ballot_sync(0xffffffffu, cls == 3);
             if (cls == 1) {
                 const int nb = __popc(mk.x) + __popc(mk.y);
-                n_inter += nb;
+                b_inter += nb;
                 if (to_list) {
                     put_entry<BPL>(list, cnt + __popc(m_one & lt), E);
                 } else if (to_m) {
@@ -519,15 +549,16 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                     const int w = xcnt + __popc(m_x & lt);
                     xlist[w] = A;
                     xmask[w] = mk;
-                    n_wrap += nb;
+                    b_wrap += nb;
                 }
             }
             cnt += __popc(m_one);
             mcnt += __popc(m_msk);
             xcnt += __popc(m_x);
             const int n_ow = __popc(m_ow), n_op = __popc(m_op);
-            if (top + 2 * n_ow + 3 * (ptop + 2 * n_op) > kXWords) {
-                overflow = true;  // children dropped (flagged)
+            if (top + 2 * n_ow + 3 * (ptop + 2 * n_op) > XW) {
+                if (REDO) overflow = true;  // children dropped (flagged)
+                else spill = true;          // the redo pass walks this bucket again
             } else {
                 if (cls == 2 && whole) {
                     const int pos = top + 2 * __popc(m_ow & lt);
@@ -536,7 +567,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                 }
                 if (cls == 2 && !whole) {
                     const int pos = ptop + 2 * __popc(m_op & lt);
-                    const int w1 = part_word(pos), w0 = part_word(pos + 1);
+                    const int w1 = part_word<XW>(pos), w0 = part_word<XW>(pos + 1);
                     stack[w1] = c1;
                     stack[w1 + 1] = (int32_t)mk.x;
                     stack[w1 + 2] = (int32_t)mk.y;
@@ -590,8 +621,9 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                 const uint32_t mw = __ballot_sync(0xffffffffu, has && whole_o);
                 const uint32_t mp = __ballot_sync(0xffffffffu, has && !whole_o);
                 const int nw = __popc(mw), npart = __popc(mp);
-                if (top + 2 * nw + 3 * (ptop + 2 * npart) > kXWords) {
-                    overflow = true;  // children dropped (flagged)
+                if (top + 2 * nw + 3 * (ptop + 2 * npart) > XW) {
+                    if (REDO) overflow = true;  // children dropped (flagged)
+                    else spill = true;          // the redo pass walks this bucket again
                 } else {
                     if (has && whole_o) {
                         const int pos = top + 2 * __popc(mw & lt);
@@ -600,7 +632,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
                     }
                     if (has && !whole_o) {
                         const int pos = ptop + 2 * __popc(mp & lt);
-                        const int w1 = part_word(pos), w0 = part_word(pos + 1);
+                        const int w1 = part_word<XW>(pos), w0 = part_word<XW>(pos + 1);
                         stack[w1] = k1c;
                         stack[w1 + 1] = (int32_t)my_om.x;
                         stack[w1 + 2] = (int32_t)my_om.y;
@@ -617,13 +649,24 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
             if (cnt >= 32) flush32<BPL, 0>(list, nullptr, cnt, lane, x, y, z, soft2, ax, ay, az);
             if (mcnt >= 32) flush32<BPL, 1>(mlist, mmask, mcnt, lane, x, y, z, soft2, ax, ay, az);
             if (xcnt >= 32) flush32<BPL, 2>(xlist, xmask, xcnt, lane, x, y, z, soft2, ax, ay, az);
+            // tests: give up on a bucket after its first round as an overflow would
+            if (TEST && rounds == 1 && g % P.test_spill_every == 0) spill = true;
+        }
+        if (!REDO && spill) {
+            // the stacks would meet: no force and no counts from this pass; the redo
+            // pass walks it again
+            if (lane == 0) table[g].w = 1;
+            __syncwarp();
+            continue;
         }
         apply_entries<BPL, false, false>(list, cnt, x, y, z, soft2, ax, ay, az);
         apply_masked<BPL, false>(mlist, mmask, mcnt, lane, x, y, z, soft2, ax, ay, az);
         apply_masked<BPL, true>(xlist, xmask, xcnt, lane, x, y, z, soft2, ax, ay, az);
         __syncwarp();
-        n_inter += n_acc;
-        n_wrap += n_acc;
+        if (REDO && lane == 0) table[g].w = 0;
+        n_tests += b_tests;
+        n_inter += b_inter + n_acc;
+        n_wrap += b_wrap + n_acc;
 #pragma unroll
         for (int b = 0; b < BPL; ++b) {
             if (valid[b]) {
@@ -653,20 +696,38 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_exact(GroupedParams P) {
     if (lane == 0) atomicMax(P.ws + 2, max_top);
 }
 
-template <int BPL, int WARPS>
-static int launch_exact_shape(GroupedParams &P, cudaStream_t st) {
-    const size_t smem = exact_smem<BPL>(WARPS);
-    CNB_CUDA(cudaFuncSetAttribute(k_forces_exact<BPL, WARPS>,
+template <int BPL, int WARPS, int XW, bool REDO, bool TEST = false>
+static int launch_exact_pass(GroupedParams &P, cudaStream_t st) {
+    const size_t smem = exact_smem<BPL>(WARPS, XW);
+    CNB_CUDA(cudaFuncSetAttribute(k_forces_exact<BPL, WARPS, XW, REDO, TEST>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_exact<BPL, WARPS>, WARPS * 32,
-                                                  smem);
-    // persistent grid: the work counter hands out buckets
-    k_forces_exact<BPL, WARPS><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_exact<BPL, WARPS, XW, REDO, TEST>,
+                                                  WARPS * 32, smem);
+    // persistent grid: the work counter (main pass) or the table scan (redo) hands out buckets
+    k_forces_exact<BPL, WARPS, XW, REDO, TEST>
+        <<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
     return launch_status();
 }
 
+template <int BPL, int WARPS>
+static int launch_exact_shape(GroupedParams &P, cudaStream_t st) {
+    // the main pass: smaller angles walk deeper and start with the wide region
+    if (P.test_spill_every > 0)  // tests: the main pass gives up on every n-th bucket
+        CNB_TRY((launch_exact_pass<BPL, WARPS, kXWords, false, true>(P, st)));
+    else if (P.theta < 0.4f)
+        CNB_TRY((launch_exact_pass<BPL, WARPS, kXWordsWide, false>(P, st)));
+    else
+        CNB_TRY((launch_exact_pass<BPL, WARPS, kXWords, false>(P, st)));
+    // the buckets it gave up on, if any (otherwise every warp scans its share of the
+    // bucket table and returns)
+    return launch_exact_pass<BPL, 2, kXWordsRedo, true>(P, st);
+}
+
+static int g_test_spill_every = 0;  // cnb_exact_test_spill
+
 int launch_exact(GroupedParams &P, int bodies_per_lane, int block_warps, cudaStream_t st) {
+    P.test_spill_every = g_test_spill_every;
     switch (bodies_per_lane * 16 + block_warps) {
         case 16 + 2: return launch_exact_shape<1, 2>(P, st);
         case 16 + 4: return launch_exact_shape<1, 4>(P, st);
@@ -679,3 +740,9 @@ int launch_exact(GroupedParams &P, int bodies_per_lane, int block_warps, cudaStr
 }
 
 }  // namespace cnb
+
+extern "C" int cnb_exact_test_spill(int every) {
+    if (every < 0) return CNB_E_INVALID_ARG;
+    cnb::g_test_spill_every = every;
+    return CNB_OK;
+}

@@ -111,9 +111,14 @@ template <int BPL, bool EWALD> __host__ __device__ constexpr int second_width() 
     return EWALD ? 3 : entry_width<BPL>();
 }
 
+// The exact minimum-image test (CNB_MAC_PERIODIC) opens every node whose
+// image box can reach a bucket and walks far wider than the other tests:
+// its node stack is this many entries per warp.
+constexpr int kGStackPeriodic = 4096;
+
 template <int BPL, bool EWALD>
-constexpr size_t grouped_smem(int warps) {
-    return (size_t)warps * (kGStack * sizeof(int32_t) +
+constexpr size_t grouped_smem(int warps, int stack) {
+    return (size_t)warps * (stack * sizeof(int32_t) +
                             kGList * (entry_width<BPL>() + second_width<BPL, EWALD>()) *
                                 sizeof(float4));
 }
@@ -187,7 +192,7 @@ __device__ __forceinline__ void apply_quad(const float4 *q, int cnt, const float
 
 // LAW: 0 the minimum-image laws (CNB_MAC_REF_X, CNB_MAC_PERIODIC), 1 the
 // periodic (Ewald) law with monopoles, 2 the periodic law with quadrupoles.
-template <int BPL, int WARPS, int LAW>
+template <int BPL, int WARPS, int LAW, int STACK>
 __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) {
     constexpr bool EWALD = LAW != 0;
     constexpr bool QUAD = LAW == 2;
@@ -203,7 +208,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
     float4 *wlist = list + kGList * EW;
     int32_t *stack =
         reinterpret_cast<int32_t *>(g_smem + WARPS * kGList * (EW + SW) * sizeof(float4)) +
-        wib * kGStack;
+        wib * STACK;
     unsigned long long n_tests = 0;
     int max_top = 0;
     bool overflow = false;
@@ -420,7 +425,7 @@ __global__ void __launch_bounds__(WARPS * 32) k_forces_grouped(GroupedParams P) 
             cnt += __popc(nm);
             wcnt += __popc(wm);
             const int nopen = __popc(om);
-            if (top + 2 * nopen > kGStack) {
+            if (top + 2 * nopen > STACK) {
                 overflow = true;  // children dropped (flagged)
             } else {
                 if (open) {
@@ -778,23 +783,26 @@ extern "C" int cnb_pack_nodes(const float *n_mass, const float *n_com, const flo
     return launch_status();
 }
 
-template <int BPL, int WARPS, int LAW>
+template <int BPL, int WARPS, int LAW, int STACK>
 static int launch_shape(GroupedParams &P, cudaStream_t st) {
-    const size_t smem = grouped_smem<BPL, LAW != 0>(WARPS);
-    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS, LAW>,
+    const size_t smem = grouped_smem<BPL, LAW != 0>(WARPS, STACK);
+    CNB_CUDA(cudaFuncSetAttribute(k_forces_grouped<BPL, WARPS, LAW, STACK>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS, LAW>, WARPS * 32,
-                                                  smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_forces_grouped<BPL, WARPS, LAW, STACK>,
+                                                  WARPS * 32, smem);
     // persistent grid: the work counter hands out buckets
-    k_forces_grouped<BPL, WARPS, LAW><<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
+    k_forces_grouped<BPL, WARPS, LAW, STACK>
+        <<<kSMs * (per_sm > 0 ? per_sm : 1), WARPS * 32, smem, st>>>(P);
     return launch_status();
 }
 
 template <int BPL, int WARPS>
 static int launch_law(GroupedParams &P, cudaStream_t st) {
-    if (P.mac != CNB_MAC_EWALD) return launch_shape<BPL, WARPS, 0>(P, st);
-    return P.quad ? launch_shape<BPL, WARPS, 2>(P, st) : launch_shape<BPL, WARPS, 1>(P, st);
+    if (P.mac == CNB_MAC_PERIODIC) return launch_shape<BPL, WARPS, 0, kGStackPeriodic>(P, st);
+    if (P.mac != CNB_MAC_EWALD) return launch_shape<BPL, WARPS, 0, kGStack>(P, st);
+    return P.quad ? launch_shape<BPL, WARPS, 2, kGStack>(P, st)
+                  : launch_shape<BPL, WARPS, 1, kGStack>(P, st);
 }
 
 static int launch_grouped(GroupedParams &P, int bodies_per_lane, int block_warps,

@@ -32,6 +32,7 @@ struct GroupedParams {
     const float4 *box_params;   // (theta, softening, slab mass, 0) per box
     int32_t *bucket_inter;      // per bucket slot: interactions of each of its bodies (may be null)
     const int32_t *bucket_order;  // the order buckets are handed out in (may be null: slot order)
+    int test_spill_every;         // exact traversal, tests only: give up on every n-th bucket
     unsigned long long *stats;  // [0] body-node interactions, [1] node tests,
                                 // [2] interactions needing the per-pair image (may be null)
     int32_t *status;

@@ -260,7 +260,8 @@ int cnb_build_tree_ranges(const uint64_t *codes, int32_t *children, int32_t *par
  * 16-byte aligned) is int32 [4 + 4N]: [0] bucket count, [1] work counter,
  * [2] deepest node stack seen by the traversal (entries; for CNB_MAC_REF_X
  * words of its stack region, one per whole-bucket entry and three per
- * part-bucket entry, of 864), [3] the bodies' (index + 1)
+ * part-bucket entry: 864 words in the main pass, 2048 for theta < 0.4, 4096
+ * when a bucket is walked again), [3] the bodies' (index + 1)
  * summed over all buckets modulo 2^32 (N(N+1)/2 when the buckets tile the
  * bodies once; cnb_upward_table_buckets flags CNB_FLAG_BAD_TOPOLOGY
  * otherwise, and also when a bucket's nodes do not form a tree over its
@@ -323,6 +324,15 @@ int cnb_forces_grouped(const float *px, const float *py, const float *pz,
                        double theta, const float *theta_per_bucket, int mac, int bodies_per_lane,
                        int block_warps, double G, double soft, double box, double slab_mass,
                        unsigned long long *stats, int32_t *status, void *stream);
+
+/* With CNB_MAC_REF_X the traversal runs in two passes: the main pass gives up
+ * on a bucket whose node stacks would outgrow its shared-memory region (it
+ * marks the bucket record's fourth word and writes no force for it), and a
+ * second pass walks only the marked buckets again with a region 4.7 times as
+ * large (two passes with the same nodes: the same forces).  Tests only:
+ * cnb_exact_test_spill(k) makes the main pass give up on every k-th bucket
+ * slot after its first round (0 = off; process-wide, not thread-safe). */
+int cnb_exact_test_spill(int every);
 
 /* Two-level form of cnb_forces_grouped (no reference counterpart; same
  * results as the one-level walk with the same mac, CNB_MAC_REF_X or

@@ -288,3 +288,45 @@ def test_super_size_change_between_builds():
     eng.check()
     assert tm.super_table_current
     _close(st.force.cpu().numpy(), f0)
+
+
+@pytest.mark.parametrize("super_bodies,theta", [(0, 0.5), (512, 0.5), (512, 0.3)])
+def test_exact_redo_pass_gives_the_same_forces(super_bodies, theta):
+    """The exact traversal's second pass: buckets the main pass gives up on (as
+    it does when their stacks would outgrow the shared region; forced here on
+    every third bucket slot after its first round) are walked again with a
+    larger region and get bit-identical forces and the same interaction
+    count; the marks are cleared afterwards."""
+    from cnb import _lib
+    from cnb.core.engine import SimulationEngine
+    from cnb.core.state import SimulationState
+    from cnb.utils import config as cfgmod
+    from cnb.utils.cosmology import zeldovich_arrays
+    cfg = cfgmod.make(N_GRID=32, SOFTENING=0.5 / 32, THETA=theta, N_STEPS=100, A_START=0.02,
+                      A_END=0.22, KEY_MODE="morton63", FORCE_MODE="grouped", BODIES_PER_LANE=2,
+                      BLOCK_WARPS=2, SUPER_BODIES=super_bodies)
+    pos, vel = zeldovich_arrays(32, 4)
+    st = SimulationState(32 ** 3, pos, vel)
+    eng = SimulationEngine(cfg, st, camera=False)
+    eng.forces_only()
+    eng.check()
+    out = []
+    for every in (0, 3, 1, 0):
+        _lib.call("cnb_exact_test_spill", every)
+        try:
+            eng.stats.zero_()
+            st.force.fill_(float("nan"))
+            eng.compute_forces()
+            eng.check()
+        finally:
+            _lib.call("cnb_exact_test_spill", 0)
+        tm = eng.tree_manager
+        nb = int(tm.workspace[0].item())
+        marks = tm.workspace[4:4 + 4 * nb].view(-1, 4)[:, 3]
+        assert int(marks.abs().sum().item()) == 0      # every mark cleared by the second pass
+        out.append((st.force.cpu().numpy().copy(), int(eng.stats[0].item())))
+    f0, c0 = out[0]
+    assert np.isfinite(f0).all()
+    for f, c in out[1:]:
+        np.testing.assert_array_equal(f.view(np.uint32), f0.view(np.uint32))
+        assert c == c0
