@@ -89,3 +89,34 @@ def test_launch_objects_reject_host_arrays():
     x = np.zeros(4, np.float32)
     with pytest.raises(TypeError):
         compute_codes[1, 256, 1](x, x, x, np.zeros(4, np.uint64), None, 4)
+
+
+def test_entry_points_of_the_fused_tree_and_training_validate_arguments():
+    """The fused build, the tensor-core gradient and the test hook reject bad
+    arguments before any device work."""
+    from cnb import _lib
+    lib = _lib.load()
+    E = _lib.CNB_E_INVALID_ARG
+    # fused build: no workspace, no root slot, bad sizes, misaligned tables
+    assert lib.cnb_build_tree_buckets(None, None, None, None, None, None, 5, 64, None, 0, None, None) == E
+    fake = 1 << 20   # never dereferenced: validation fails first
+    assert lib.cnb_build_tree_buckets(None, None, None, None, None, fake, 5, 64, fake, 0, None, None) == E
+    assert lib.cnb_build_tree_buckets(fake, fake, fake, fake, fake, fake, 5, 0, fake, 0, None, None) == E
+    assert lib.cnb_build_tree_buckets(fake, fake, fake, fake, fake, fake, 5, 64, fake, 0, fake, None) == E
+    assert lib.cnb_build_tree_buckets(fake, fake, fake, fake + 4, fake, fake, 5, 64, fake, 512, fake,
+                                      None) == E
+    assert lib.cnb_build_tree_buckets(fake, fake, fake, fake, fake, fake, -1, 64, fake, 0, None, None) == E
+    # tensor-core gradient: scratch size and alignment
+    assert lib.cnb_mlp_grad_mma_scratch_bytes(0) == -1
+    assert lib.cnb_mlp_grad_mma_scratch_bytes(1) == 416 * 32
+    assert lib.cnb_mlp_grad_mma_scratch_bytes(33) == 416 * 64
+    nb = lib.cnb_mlp_grad_mma_scratch_bytes(100)
+    assert lib.cnb_mlp_grad_mma(fake, fake, 100, fake, 1.0, fake, nb - 16, fake, fake, None) == E
+    assert lib.cnb_mlp_grad_mma(fake, fake, 100, fake, 1.0, fake + 8, nb, fake, fake, None) == E
+    assert lib.cnb_mlp_grad_mma(fake, fake, 0, fake, 1.0, fake, nb, fake, fake, None) == E
+    # the exact traversal's test hook
+    assert lib.cnb_exact_test_spill(-1) == E
+    assert lib.cnb_exact_test_spill(0) == _lib.CNB_OK
+    # two-level forces: ranges and parents both given or both NULL (prebuilt table)
+    assert lib.cnb_forces_two_level(fake, fake, fake, fake, fake, None, fake, fake, 1 << 30, 512, fake,
+                                    5, 0.5, 0, 2, 2, 1.0, 0.01, 1.0, None, None, None) == E
