@@ -41,6 +41,10 @@
 // lane j keeps item j's mask of opening bodies and the children of a round's
 // items are pushed together after them.
 //
+// The node stacks live in shared memory (see kXWords); a bucket that would
+// outgrow them in the main pass is walked again by a second launch with a
+// larger region, so deep walks keep their exact node sets.
+//
 // Limit: the reference's 64-entry stack drops children when full
 // (physics_kernels.py:143-149).  That happens only for trees deeper than
 // about 63 levels; the exact walk has no such drop.
