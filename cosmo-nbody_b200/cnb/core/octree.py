@@ -10,6 +10,11 @@ and a float64 root, `self.root_f64` = [mass, com x, y, z]), and
 `node_table=True`, which also builds what the grouped force traversal reads:
 the node table (`self.node_table`, [4, M, 4] float32), the node ranges and
 the bucket table (`self.workspace`, buckets of at most `bucket` bodies).
+With the plain upward pass and buckets of at most 64 bodies the tree is two
+launches: the Karras build fused with the ranges, climb counters, root index
+and bucket tables (and the super-bucket table of `set_super_table`), then
+the bucketed upward pass; the reference-layout arrays are then filled from
+the node table when `get_buffers()` asks for them.
 """
 from __future__ import annotations
 
