@@ -69,9 +69,15 @@ def test_lagrangian_allocation_meets_the_global_budget():
     assert v <= allowed
     assert total <= costs[1].sum() + 1e-9
     best = np.inf
+    best_at_v = np.inf     # the cheapest allocation with no more violations than the one returned
     for choice in itertools.product(range(T), repeat=G):
         c = np.array(choice)
         viol = sum(int((errors[c[g], owner == g] > budget).sum()) for g in range(G))
+        cost = costs[c, np.arange(G)].sum()
         if viol <= allowed:
-            best = min(best, costs[c, np.arange(G)].sum())
+            best = min(best, cost)
+        if viol <= v:
+            best_at_v = min(best_at_v, cost)
     assert total <= best * 1.15       # the Lagrangian point is close to the exhaustive optimum
+    # and it is exactly the cheapest allocation with at most its own violations
+    assert abs(total - best_at_v) <= 1e-9 * best_at_v
